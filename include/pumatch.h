@@ -1,0 +1,239 @@
+/*
+ * pumatch.h -- C-ABI of libpumatch_b200.so, a B200-native subgraph matcher.
+ *
+ * The reference (PUMatch) has no library API: its boundary is the CLI
+ * `test <graph-prefix> <pattern.g>` (test.cu:15-21) plus three header-only
+ * host classes (GraphPreprocessor, PatternPreprocessor, JobQueuePreprocessor)
+ * and one kernel `_parallel_match` (src/gpu_match.cuh:10-13).  Each entry point
+ * below names the reference piece it replaces.  All signatures use plain
+ * pointers and sizes; no C++ or torch types cross this boundary.
+ *
+ * Ownership: every handle is owned by the caller and freed by the matching
+ * *_close / *_free / *_destroy call.  Output buffers are caller-owned.
+ * Errors: every call returns a pm_status; pm_last_error() gives a message for
+ * the calling thread.  No call exits the process (the reference calls exit(1)
+ * on a missing file, src/graph.h:216-226).
+ */
+#ifndef PUMATCH_H
+#define PUMATCH_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  PM_OK = 0,
+  PM_ERR_IO = 1,        /* file missing or unreadable                          */
+  PM_ERR_FORMAT = 2,    /* malformed .meta/.bin/.g content                     */
+  PM_ERR_OOM = 3,       /* host or device allocation failed                    */
+  PM_ERR_CUDA = 4,      /* a CUDA runtime call failed                          */
+  PM_ERR_TIMEOUT = 5,   /* a bounded device wait gave up (status word)         */
+  PM_ERR_INVALID = 6,   /* bad argument                                        */
+  PM_ERR_INTERNAL = 7,  /* device-side check failed (arena/overflow/etc.)      */
+  PM_ERR_NO_DEVICE = 8  /* no CUDA device; the product has no CPU fallback     */
+} pm_status;
+
+typedef struct pm_graph pm_graph; /* CSR graph placed for matching          */
+typedef struct pm_plan pm_plan;   /* compiled pattern                        */
+typedef struct pm_ctx pm_ctx;     /* device, streams, scratch arenas         */
+
+/* ------------------------------------------------------------------ */
+/* Graph                                                                */
+/* ------------------------------------------------------------------ */
+
+enum {
+  PM_RESIDENT_HBM = 0,   /* whole CSR copied to device memory                  */
+  PM_RESIDENT_PAGED = 1  /* adjacency stays in pinned host memory; a device
+                            frame pool caches fixed-size pages of it           */
+};
+
+typedef struct {
+  int labeled;              /* 1: read .label.bin (reference LABELED=true)     */
+  int device;               /* CUDA ordinal                                    */
+  int residency;            /* PM_RESIDENT_*                                   */
+  uint32_t page_bytes;      /* paged mode: page size (multiple of 4 KiB)       */
+  uint64_t frame_pool_bytes;/* paged mode: device frame-pool cap               */
+} pm_graph_opts;
+
+typedef struct {
+  int64_t n_vertices;
+  int64_t n_adj;            /* adjacency entries = 2 x undirected edges        */
+  int32_t max_degree;
+  int32_t labeled;
+  int32_t n_labels;         /* 1 + max label value (labeled graphs)            */
+  int32_t residency;
+  uint64_t device_bytes;    /* device memory held by the graph                 */
+  uint64_t n_pages;         /* paged mode: pages of the adjacency array        */
+  uint64_t n_frames;        /* paged mode: frames in the device pool           */
+} pm_graph_info;
+
+void pm_graph_opts_default(pm_graph_opts* o);
+
+/* Replaces GraphPreprocessor(prefix) + to_gpu()/to_gpu_managed()
+ * (src/graph.h:34-41, 169-208, 228-254): reads <prefix>.meta.txt, .vertex.bin,
+ * .edge.bin and, when labeled, .label.bin, and places the graph on the device. */
+pm_status pm_graph_open(const char* prefix, const pm_graph_opts* opts, pm_graph** out);
+
+/* Same placement from caller-owned HOST arrays (rowptr: n+1 uint64, colidx:
+ * n_adj int32 sorted per list, labels: n uint32 or NULL).  The arrays are
+ * copied; the caller keeps ownership. */
+pm_status pm_graph_from_host(int64_t n, int64_t n_adj, const uint64_t* rowptr,
+                             const int32_t* colidx, const uint32_t* labels,
+                             const pm_graph_opts* opts, pm_graph** out);
+
+/* Wrap DEVICE arrays already resident in HBM (rowptr uint64[n+1], colidx
+ * int32[n_adj], labels uint8[n] or NULL).  Nothing is copied and the graph does
+ * not own them; max_degree must be exact. */
+pm_status pm_graph_from_device(int64_t n, int64_t n_adj, int32_t max_degree,
+                               const uint64_t* d_rowptr, const int32_t* d_colidx,
+                               const uint8_t* d_labels, int device, pm_graph** out);
+
+pm_status pm_graph_get_info(const pm_graph* g, pm_graph_info* info);
+void pm_graph_close(pm_graph* g);
+
+/* Reader/writer of the reference's on-disk layout (src/graph.h:228-254,
+ * graph_converter/compactify.cpp:40-48, labelize.cpp:41-50) for host arrays.
+ * pm_graph_read allocates *rowptr/*colidx/*labels with malloc; free with
+ * pm_host_free. */
+pm_status pm_graph_read(const char* prefix, int labeled, int64_t* n, int64_t* n_adj,
+                        int32_t* max_degree, uint64_t** rowptr, int32_t** colidx,
+                        uint32_t** labels);
+pm_status pm_graph_write(const char* prefix, int64_t n, int64_t n_adj,
+                         const uint64_t* rowptr, const int32_t* colidx,
+                         const uint32_t* labels);
+void pm_host_free(void* p);
+
+/* ------------------------------------------------------------------ */
+/* Synthetic inputs (stand-ins for the reference's converted datasets)  */
+/* ------------------------------------------------------------------ */
+
+/* Seeded Chung-Lu graph: expected degree w_i = c*(i+i0)^(-1/(gamma-1)) scaled
+ * to sum 2*n_edges and capped at max_w; endpoints sampled with probability
+ * proportional to w; self-loops and duplicates dropped and topped up until
+ * exactly n_edges unique undirected edges.  Output CSR is malloc'd. */
+pm_status pm_gen_chung_lu(int64_t n, int64_t n_edges, double gamma, double i0,
+                          double max_w, uint64_t seed, uint64_t** rowptr,
+                          int32_t** colidx, int64_t* n_adj, int32_t* max_degree);
+
+/* Seeded R-MAT graph (a,b,c,d quadrant probabilities, ids >= n rejected),
+ * n_edges unique undirected non-loop edges. */
+pm_status pm_gen_rmat(int64_t n, int64_t n_edges, double a, double b, double c,
+                      uint64_t seed, uint64_t** rowptr, int32_t** colidx,
+                      int64_t* n_adj, int32_t* max_degree);
+
+/* Uniform labels in [0, n_labels) (malloc'd uint32[n]). */
+pm_status pm_gen_labels(int64_t n, int n_labels, uint64_t seed, uint32_t** labels);
+
+/* ------------------------------------------------------------------ */
+/* Pattern plans                                                        */
+/* ------------------------------------------------------------------ */
+
+#define PM_MAX_PAT 7
+#define PM_MAX_SLOTS 15
+
+/* Flattened plan, the kernel's contract (same content as the reference's
+ * `Pattern` struct, src/pattern.h:17-25, plus the multiplicity). */
+typedef struct {
+  int32_t nnodes;
+  int32_t nslots;
+  int32_t multiplicity;               /* |Aut(P)| (PatternMultiplicity)     */
+  int32_t labeled;
+  int32_t level_begin[PM_MAX_PAT + 1];/* rowptr: slots of level L are
+                                         [level_begin[L], level_begin[L+1]) */
+  int32_t degree[PM_MAX_PAT];
+  int32_t vertex_label[PM_MAX_PAT];   /* pattern labels (1 when unlabeled)  */
+  uint32_t slot_labels[PM_MAX_SLOTS]; /* one-hot label mask per slot        */
+  uint32_t partial[PM_MAX_SLOTS];     /* symmetry-breaking bits per slot    */
+  uint8_t set_ops[PM_MAX_SLOTS];      /* 0x20 fresh, 0x40 intersect, else
+                                         copy; low 5 bits = parent slot     */
+  uint8_t pad_[1];
+} pm_plan_desc;
+
+/* Replaces PatternPreprocessor(file) (src/pattern.h:48-58). */
+pm_status pm_plan_compile(const char* g_path, int labeled, pm_plan** out);
+pm_status pm_plan_compile_text(const char* g_text, int labeled, pm_plan** out);
+pm_status pm_plan_describe(const pm_plan* p, pm_plan_desc* out);
+void pm_plan_free(pm_plan* p);
+
+/* Replaces JobQueuePreprocessor(g, p) (src/job_queue.h:39-64): counts the
+ * root edges that pass the reference's filters (computed on the GPU). */
+pm_status pm_count_roots(pm_ctx* ctx, const pm_graph* g, const pm_plan* p, int64_t* n_roots);
+
+/* Copies the root list of one plan (pairs r,c in reference order, up to cap
+ * pairs) and its length: the same list JobQueuePreprocessor builds, for
+ * parity checks of the GPU root filter. */
+pm_status pm_debug_roots(pm_ctx* ctx, const pm_graph* g, const pm_plan* p, int32_t* out_pairs,
+                         int64_t cap, int64_t* n_roots);
+
+/* ------------------------------------------------------------------ */
+/* Matching                                                             */
+/* ------------------------------------------------------------------ */
+
+pm_status pm_ctx_create(int device, pm_ctx** out);
+void pm_ctx_destroy(pm_ctx* ctx);
+
+typedef struct {
+  int32_t truncate;         /* 0: exact.  >0: emulate the reference's
+                               GRAPH_DEGREE truncation of every set result
+                               (src/gpu_match.cu:302,316); 4096 as shipped    */
+  int32_t warps_per_block;  /* 0 = default                                  */
+  int32_t blocks_per_sm;    /* 0 = default                                  */
+  int32_t chunk;            /* root edges per queue pop; 0 = default         */
+  int32_t split_level1;     /* >0: donate level-1 ranges of at least this
+                               many candidates to idle warps; 0 = default;
+                               -1 = never split                              */
+  int32_t shard_rank;       /* multi-GPU root sharding: this shard (0-based) */
+  int32_t shard_count;      /* number of shards; 0/1 = no sharding; shard k
+                               takes root chunks k, k+count, ...            */
+  int32_t use_graph;        /* 1: capture the launch in a CUDA graph         */
+  int32_t timeout_ms;       /* bound on every device wait; 0 = default       */
+  int64_t root_begin;       /* restrict to roots [root_begin, root_end) of
+                               the reference-ordered root list; -1 = all     */
+  int64_t root_end;
+  int32_t reserved_[4];
+  uint64_t* root_counts;    /* optional device ptr: per-root counts (plan 0) */
+  float* root_cost;         /* optional device ptr: per-root set-op bytes    */
+  const int32_t* root_order;/* optional device ptr: process roots in this
+                               order (learned binning); NULL = natural      */
+} pm_run_opts;
+
+void pm_run_opts_default(pm_run_opts* o);
+
+typedef struct {
+  uint64_t n_roots;         /* root edges processed (all plans)             */
+  uint64_t set_ops;         /* executed set operations                      */
+  uint64_t alg_bytes;       /* sum over set ops of 4(|A|+|B|+|C|) (+|A|
+                               label bytes when labeled) + 8 per root       */
+  uint64_t splits;          /* level-1 ranges donated between warps         */
+  uint64_t page_hits;       /* paged mode: adjacency reads served from HBM  */
+  uint64_t page_misses;     /* paged mode: reads served over the host link  */
+  uint64_t h2d_page_bytes;  /* paged mode: bytes copied into frames         */
+  uint64_t zero_copy_bytes; /* paged mode: bytes read directly from host    */
+  uint64_t pages_loaded;
+  uint64_t evictions;
+  float kernel_ms;          /* device time of the matching launch(es)       */
+  float roots_ms;           /* device time of the root filter               */
+  int32_t grid_blocks;
+  int32_t block_threads;
+  uint64_t arena_bytes;
+  uint32_t device_status;   /* 0 ok; else PM_DEV_* flags                     */
+  uint32_t pad_;
+} pm_stats;
+
+/* Replaces the `_parallel_match` launch and the host reduction of per-warp
+ * counts (test.cu:171-198).  Runs every plan over the graph in one persistent
+ * launch and writes one exact count per plan (multiplied by the pattern's
+ * automorphism count when unlabeled, as test.cu:198 does). */
+pm_status pm_match(pm_ctx* ctx, const pm_graph* g, const pm_plan* const* plans, int nplans,
+                   const pm_run_opts* opts, uint64_t* counts_out, pm_stats* stats_out);
+
+const char* pm_strerror(pm_status s);
+const char* pm_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PUMATCH_H */

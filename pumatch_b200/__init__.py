@@ -1,0 +1,399 @@
+"""pumatch_b200 -- B200-native subgraph matcher.
+
+Host-side mirror of the reference's driver interface (PUMatch ``test.cu`` and
+its header-only preprocessors) over the C-ABI of ``libpumatch_b200.so``:
+
+    GraphPreprocessor(prefix)          -> reference src/graph.h:34-41
+    PatternPreprocessor(path)          -> reference src/pattern.h:48-58
+    count_roots(graph, pattern)        -> reference src/job_queue.h:39-64
+    match(graph, patterns, ...)        -> reference test.cu:171-198
+
+Every call goes through the compiled library; there is no Python or CPU
+fallback.  If the library is missing, importing the matcher API raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Iterable, Optional, Sequence
+
+import numpy as np
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_PKG, "lib", "libpumatch_b200.so")
+CLI_PATH = os.path.join(_PKG, "bin", "test")
+
+PM_OK, PM_ERR_IO, PM_ERR_FORMAT, PM_ERR_OOM, PM_ERR_CUDA = 0, 1, 2, 3, 4
+PM_ERR_TIMEOUT, PM_ERR_INVALID, PM_ERR_INTERNAL, PM_ERR_NO_DEVICE = 5, 6, 7, 8
+PM_RESIDENT_HBM, PM_RESIDENT_PAGED = 0, 1
+MAX_PAT, MAX_SLOTS = 7, 15
+
+
+class PmError(RuntimeError):
+    """A non-OK pm_status, with the library's message for this thread."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(f"[{status}] {message}")
+        self.status = status
+        self.message = message
+
+
+class GraphOpts(C.Structure):
+    _fields_ = [("labeled", C.c_int), ("device", C.c_int), ("residency", C.c_int),
+                ("page_bytes", C.c_uint32), ("frame_pool_bytes", C.c_uint64)]
+
+
+class GraphInfo(C.Structure):
+    _fields_ = [("n_vertices", C.c_int64), ("n_adj", C.c_int64), ("max_degree", C.c_int32),
+                ("labeled", C.c_int32), ("n_labels", C.c_int32), ("residency", C.c_int32),
+                ("device_bytes", C.c_uint64), ("n_pages", C.c_uint64), ("n_frames", C.c_uint64)]
+
+
+class PlanDesc(C.Structure):
+    _fields_ = [("nnodes", C.c_int32), ("nslots", C.c_int32), ("multiplicity", C.c_int32),
+                ("labeled", C.c_int32), ("level_begin", C.c_int32 * (MAX_PAT + 1)),
+                ("degree", C.c_int32 * MAX_PAT), ("vertex_label", C.c_int32 * MAX_PAT),
+                ("slot_labels", C.c_uint32 * MAX_SLOTS), ("partial", C.c_uint32 * MAX_SLOTS),
+                ("set_ops", C.c_uint8 * MAX_SLOTS), ("pad_", C.c_uint8)]
+
+
+class RunOpts(C.Structure):
+    _fields_ = [("truncate", C.c_int32), ("warps_per_block", C.c_int32), ("blocks_per_sm", C.c_int32),
+                ("chunk", C.c_int32), ("split_level1", C.c_int32), ("shard_rank", C.c_int32),
+                ("shard_count", C.c_int32), ("use_graph", C.c_int32), ("timeout_ms", C.c_int32),
+                ("root_begin", C.c_int64), ("root_end", C.c_int64), ("reserved_", C.c_int32 * 4),
+                ("root_counts", C.c_void_p), ("root_cost", C.c_void_p), ("root_order", C.c_void_p)]
+
+
+class Stats(C.Structure):
+    _fields_ = [("n_roots", C.c_uint64), ("set_ops", C.c_uint64), ("alg_bytes", C.c_uint64),
+                ("splits", C.c_uint64), ("page_hits", C.c_uint64), ("page_misses", C.c_uint64),
+                ("h2d_page_bytes", C.c_uint64), ("zero_copy_bytes", C.c_uint64),
+                ("pages_loaded", C.c_uint64), ("evictions", C.c_uint64), ("kernel_ms", C.c_float),
+                ("roots_ms", C.c_float), ("grid_blocks", C.c_int32), ("block_threads", C.c_int32),
+                ("arena_bytes", C.c_uint64), ("device_status", C.c_uint32), ("pad_", C.c_uint32)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_ if not k.endswith("_")}
+
+
+_lib = None
+
+# name -> (restype, argtypes) of every C-ABI entry point in include/pumatch.h
+_P = C.c_void_p
+_PP = C.POINTER(C.c_void_p)
+SIGNATURES = {
+    "pm_graph_opts_default": (None, [C.POINTER(GraphOpts)]),
+    "pm_graph_open": (C.c_int, [C.c_char_p, C.POINTER(GraphOpts), _PP]),
+    "pm_graph_from_host": (C.c_int, [C.c_int64, C.c_int64, _P, _P, _P, C.POINTER(GraphOpts), _PP]),
+    "pm_graph_from_device": (C.c_int, [C.c_int64, C.c_int64, C.c_int32, _P, _P, _P, C.c_int, _PP]),
+    "pm_graph_get_info": (C.c_int, [_P, C.POINTER(GraphInfo)]),
+    "pm_graph_close": (None, [_P]),
+    "pm_graph_read": (C.c_int, [C.c_char_p, C.c_int, C.POINTER(C.c_int64), C.POINTER(C.c_int64),
+                                C.POINTER(C.c_int32), _PP, _PP, _PP]),
+    "pm_graph_write": (C.c_int, [C.c_char_p, C.c_int64, C.c_int64, _P, _P, _P]),
+    "pm_host_free": (None, [_P]),
+    "pm_gen_chung_lu": (C.c_int, [C.c_int64, C.c_int64, C.c_double, C.c_double, C.c_double, C.c_uint64,
+                                  _PP, _PP, C.POINTER(C.c_int64), C.POINTER(C.c_int32)]),
+    "pm_gen_rmat": (C.c_int, [C.c_int64, C.c_int64, C.c_double, C.c_double, C.c_double, C.c_uint64,
+                              _PP, _PP, C.POINTER(C.c_int64), C.POINTER(C.c_int32)]),
+    "pm_gen_labels": (C.c_int, [C.c_int64, C.c_int, C.c_uint64, _PP]),
+    "pm_plan_compile": (C.c_int, [C.c_char_p, C.c_int, _PP]),
+    "pm_plan_compile_text": (C.c_int, [C.c_char_p, C.c_int, _PP]),
+    "pm_plan_describe": (C.c_int, [_P, C.POINTER(PlanDesc)]),
+    "pm_plan_free": (None, [_P]),
+    "pm_count_roots": (C.c_int, [_P, _P, _P, C.POINTER(C.c_int64)]),
+    "pm_debug_roots": (C.c_int, [_P, _P, _P, _P, C.c_int64, C.POINTER(C.c_int64)]),
+    "pm_ctx_create": (C.c_int, [C.c_int, _PP]),
+    "pm_ctx_destroy": (None, [_P]),
+    "pm_run_opts_default": (None, [C.POINTER(RunOpts)]),
+    "pm_match": (C.c_int, [_P, _P, _PP, C.c_int, C.POINTER(RunOpts), C.POINTER(C.c_uint64),
+                           C.POINTER(Stats)]),
+    "pm_strerror": (C.c_char_p, [C.c_int]),
+    "pm_last_error": (C.c_char_p, []),
+}
+
+
+def lib() -> C.CDLL:
+    """Loads libpumatch_b200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: run `python -m pumatch_b200.build` "
+                              "(there is no fallback implementation)")
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _check(status: int) -> None:
+    if status != PM_OK:
+        raise PmError(status, lib().pm_last_error().decode(errors="replace"))
+
+
+def _ptr(a: Optional[np.ndarray]):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def _take(ptr: C.c_void_p, n: int, dtype) -> np.ndarray:
+    """Copies n elements of a malloc'd array into numpy and frees it."""
+    if n == 0:
+        lib().pm_host_free(ptr)
+        return np.zeros(0, dtype=dtype)
+    buf = (C.c_char * (n * np.dtype(dtype).itemsize)).from_address(ptr.value)
+    out = np.frombuffer(buf, dtype=dtype).copy()
+    lib().pm_host_free(ptr)
+    return out
+
+
+# ---------------------------------------------------------------- host CSR
+
+class HostGraph:
+    """CSR arrays in host memory in the reference's on-disk layout."""
+
+    def __init__(self, rowptr: np.ndarray, colidx: np.ndarray, labels: Optional[np.ndarray] = None):
+        self.rowptr = np.ascontiguousarray(rowptr, dtype=np.uint64)
+        self.colidx = np.ascontiguousarray(colidx, dtype=np.int32)
+        self.labels = None if labels is None else np.ascontiguousarray(labels, dtype=np.uint32)
+
+    @property
+    def n(self) -> int:
+        return len(self.rowptr) - 1
+
+    @property
+    def n_adj(self) -> int:
+        return len(self.colidx)
+
+    @property
+    def max_degree(self) -> int:
+        return int(np.diff(self.rowptr).max()) if self.n else 0
+
+    def degrees(self) -> np.ndarray:
+        return np.diff(self.rowptr).astype(np.int64)
+
+    def write(self, prefix: str) -> None:
+        """Writes <prefix>.meta.txt/.vertex.bin/.edge.bin[/.label.bin]."""
+        _check(lib().pm_graph_write(prefix.encode(), self.n, self.n_adj, _ptr(self.rowptr),
+                                    _ptr(self.colidx), _ptr(self.labels)))
+
+    @staticmethod
+    def read(prefix: str, labeled: bool) -> "HostGraph":
+        n, nadj, md = C.c_int64(), C.c_int64(), C.c_int32()
+        rp, ci, lb = C.c_void_p(), C.c_void_p(), C.c_void_p()
+        _check(lib().pm_graph_read(prefix.encode(), int(labeled), C.byref(n), C.byref(nadj), C.byref(md),
+                                   C.byref(rp), C.byref(ci), C.byref(lb)))
+        rowptr = _take(rp, n.value + 1, np.uint64)
+        colidx = _take(ci, nadj.value, np.int32)
+        labels = _take(lb, n.value, np.uint32) if labeled else None
+        return HostGraph(rowptr, colidx, labels)
+
+
+def gen_chung_lu(n: int, n_edges: int, gamma: float = 2.1, i0: float = 10.0, max_w: float = 5000.0,
+                 seed: int = 1) -> HostGraph:
+    """Seeded Chung-Lu power-law graph (sorted, deduplicated, no self-loops)."""
+    rp, ci, nadj, md = C.c_void_p(), C.c_void_p(), C.c_int64(), C.c_int32()
+    _check(lib().pm_gen_chung_lu(n, n_edges, gamma, i0, max_w, seed, C.byref(rp), C.byref(ci),
+                                 C.byref(nadj), C.byref(md)))
+    return HostGraph(_take(rp, n + 1, np.uint64), _take(ci, nadj.value, np.int32))
+
+
+def gen_rmat(n: int, n_edges: int, a: float = 0.57, b: float = 0.19, c: float = 0.19,
+             seed: int = 2) -> HostGraph:
+    """Seeded R-MAT graph (ids >= n rejected; sorted, deduplicated, no self-loops)."""
+    rp, ci, nadj, md = C.c_void_p(), C.c_void_p(), C.c_int64(), C.c_int32()
+    _check(lib().pm_gen_rmat(n, n_edges, a, b, c, seed, C.byref(rp), C.byref(ci), C.byref(nadj),
+                             C.byref(md)))
+    return HostGraph(_take(rp, n + 1, np.uint64), _take(ci, nadj.value, np.int32))
+
+
+def gen_labels(n: int, n_labels: int, seed: int) -> np.ndarray:
+    lb = C.c_void_p()
+    _check(lib().pm_gen_labels(n, n_labels, seed, C.byref(lb)))
+    return _take(lb, n, np.uint32)
+
+
+# ---------------------------------------------------------------- patterns
+
+class PatternPreprocessor:
+    """A compiled pattern plan (reference src/pattern.h:48-58)."""
+
+    def __init__(self, path: Optional[str] = None, *, text: Optional[str] = None, labeled: bool = True):
+        h = C.c_void_p()
+        if text is not None:
+            _check(lib().pm_plan_compile_text(text.encode(), int(labeled), C.byref(h)))
+        elif path is not None:
+            _check(lib().pm_plan_compile(path.encode(), int(labeled), C.byref(h)))
+        else:
+            raise ValueError("give a .g path or text=")
+        self._h = h
+        self.path = path
+        self.labeled = labeled
+
+    def describe(self) -> dict:
+        d = PlanDesc()
+        _check(lib().pm_plan_describe(self._h, C.byref(d)))
+        n, ns = d.nnodes, d.nslots
+        return {
+            "labeled": d.labeled, "nnodes": n, "multiplicity": d.multiplicity, "nslots": ns,
+            "level_begin": list(d.level_begin)[:n], "degree": list(d.degree)[:n],
+            "vertex_label": list(d.vertex_label)[:n], "partial": list(d.partial)[:ns],
+            "slot_labels": [0] + list(d.slot_labels)[1:ns], "set_ops": [0] + list(d.set_ops)[1:ns],
+        }
+
+    @property
+    def PatternMultiplicity(self) -> int:  # noqa: N802 -- reference spelling
+        return self.describe()["multiplicity"]
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib().pm_plan_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ---------------------------------------------------------------- device graph
+
+class GraphPreprocessor:
+    """A CSR graph placed on the device (reference src/graph.h:34-41, 169-208).
+
+    ``GraphPreprocessor(prefix)`` reads the reference's file layout;
+    ``GraphPreprocessor.from_host(HostGraph)`` places in-memory arrays.
+    """
+
+    def __init__(self, prefix: Optional[str] = None, *, labeled: bool = True, device: int = 0,
+                 paged: bool = False, frame_pool_bytes: int = 4 << 30, page_bytes: int = 64 << 10,
+                 _handle=None):
+        self._h = None
+        if _handle is not None:
+            self._h = _handle
+            return
+        o = self._opts(labeled, device, paged, frame_pool_bytes, page_bytes)
+        h = C.c_void_p()
+        _check(lib().pm_graph_open(prefix.encode(), C.byref(o), C.byref(h)))
+        self._h = h
+
+    @staticmethod
+    def _opts(labeled, device, paged, frame_pool_bytes, page_bytes) -> GraphOpts:
+        o = GraphOpts()
+        lib().pm_graph_opts_default(C.byref(o))
+        o.labeled = int(labeled)
+        o.device = device
+        o.residency = PM_RESIDENT_PAGED if paged else PM_RESIDENT_HBM
+        o.frame_pool_bytes = frame_pool_bytes
+        o.page_bytes = page_bytes
+        return o
+
+    @classmethod
+    def from_host(cls, hg: HostGraph, *, labeled: bool = False, device: int = 0, paged: bool = False,
+                  frame_pool_bytes: int = 4 << 30, page_bytes: int = 64 << 10) -> "GraphPreprocessor":
+        o = cls._opts(labeled, device, paged, frame_pool_bytes, page_bytes)
+        h = C.c_void_p()
+        _check(lib().pm_graph_from_host(hg.n, hg.n_adj, _ptr(hg.rowptr), _ptr(hg.colidx),
+                                        _ptr(hg.labels) if labeled else None, C.byref(o), C.byref(h)))
+        return cls(_handle=h)
+
+    @classmethod
+    def from_device(cls, n: int, n_adj: int, max_degree: int, rowptr_ptr: int, colidx_ptr: int,
+                    labels_ptr: Optional[int], device: int = 0) -> "GraphPreprocessor":
+        h = C.c_void_p()
+        _check(lib().pm_graph_from_device(n, n_adj, max_degree, C.c_void_p(rowptr_ptr), C.c_void_p(colidx_ptr),
+                                          C.c_void_p(labels_ptr) if labels_ptr else None, device, C.byref(h)))
+        return cls(_handle=h)
+
+    def info(self) -> dict:
+        gi = GraphInfo()
+        _check(lib().pm_graph_get_info(self._h, C.byref(gi)))
+        return {k: getattr(gi, k) for k, _ in gi._fields_}
+
+    def close(self) -> None:
+        if self._h:
+            lib().pm_graph_close(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Context:
+    """Device, streams and reusable scratch (one per host thread)."""
+
+    def __init__(self, device: int = 0):
+        h = C.c_void_p()
+        _check(lib().pm_ctx_create(device, C.byref(h)))
+        self._h = h
+        self.device = device
+
+    def close(self) -> None:
+        if self._h:
+            lib().pm_ctx_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def count_roots(self, g: GraphPreprocessor, p: PatternPreprocessor) -> int:
+        n = C.c_int64()
+        _check(lib().pm_count_roots(self._h, g._h, p._h, C.byref(n)))
+        return n.value
+
+    def roots(self, g: GraphPreprocessor, p: PatternPreprocessor) -> np.ndarray:
+        """The root list (reference Job[] order) as an (n, 2) int32 array."""
+        n = self.count_roots(g, p)
+        out = np.zeros((max(n, 1), 2), dtype=np.int32)
+        got = C.c_int64()
+        _check(lib().pm_debug_roots(self._h, g._h, p._h, _ptr(out), n, C.byref(got)))
+        return out[:n]
+
+    def match(self, g: GraphPreprocessor, patterns: Sequence[PatternPreprocessor], *, truncate: int = 0,
+              warps_per_block: int = 0, blocks_per_sm: int = 0, chunk: int = 0, split_level1: int = 0,
+              shard_rank: int = 0, shard_count: int = 0, root_begin: int = -1, root_end: int = -1,
+              root_counts_ptr: int = 0, root_cost_ptr: int = 0, root_order_ptr: int = 0,
+              use_graph: bool = False):
+        """Runs all patterns in one launch; returns (counts list, stats dict)."""
+        o = RunOpts()
+        lib().pm_run_opts_default(C.byref(o))
+        o.truncate, o.warps_per_block, o.blocks_per_sm, o.chunk = truncate, warps_per_block, blocks_per_sm, chunk
+        o.split_level1, o.shard_rank, o.shard_count = split_level1, shard_rank, shard_count
+        o.root_begin, o.root_end, o.use_graph = root_begin, root_end, int(use_graph)
+        o.root_counts = root_counts_ptr or None
+        o.root_cost = root_cost_ptr or None
+        o.root_order = root_order_ptr or None
+        k = len(patterns)
+        arr = (C.c_void_p * k)(*[p._h.value for p in patterns])
+        counts = (C.c_uint64 * k)()
+        st = Stats()
+        _check(lib().pm_match(self._h, g._h, C.cast(arr, _PP), k, C.byref(o), counts, C.byref(st)))
+        return [int(x) for x in counts], st.as_dict()
+
+
+def match(g: GraphPreprocessor, patterns, ctx: Optional[Context] = None, **kw):
+    """Counts every pattern in one persistent launch (reference test.cu:171-198)."""
+    own = ctx is None
+    ctx = ctx or Context(0)
+    try:
+        pats = patterns if isinstance(patterns, (list, tuple)) else [patterns]
+        return ctx.match(g, pats, **kw)
+    finally:
+        if own:
+            ctx.close()
+
+
+__all__ = [
+    "PmError", "HostGraph", "GraphPreprocessor", "PatternPreprocessor", "Context", "match",
+    "gen_chung_lu", "gen_rmat", "gen_labels", "lib", "LIB_PATH", "CLI_PATH", "SIGNATURES",
+]

@@ -1,0 +1,115 @@
+// pm_cli.cpp -- the drop-in `test` command.
+//
+//   test <graph-prefix> <pattern.g> [--labeled=0|1] [--truncate=N] [--device=D]
+//        [--paged] [--frame-mb=M] [--page-kb=K] [--batch=<list file>]
+//
+// Same positional arguments and output as the reference's driver
+// (test.cu:15-21, 200-209): the last stdout line is "<kernel ms> <count>" and
+// "<graph>\t<pattern>\t<ms>\t<count>" is appended to ./result.txt.
+// Diagnostics go to stderr.  Defaults follow the reference as shipped:
+// labeled matching (src/config.h:14); exact candidate sets unless
+// --truncate=4096 asks for the reference's GRAPH_DEGREE cap.
+// With --batch, <pattern.g> is ignored and each line of the list file names a
+// pattern; all run in one launch and one "<ms> <count>" line is printed per
+// pattern in list order (ms is the shared launch time).
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <iostream>
+#include <string>
+#include <vector>
+
+#include "pumatch.h"
+
+static int die(const char* what, pm_status s) {
+  fprintf(stderr, "test: %s: %s (%s)\n", what, pm_strerror(s), pm_last_error());
+  return 1;
+}
+
+int main(int argc, char** argv) {
+  if (argc < 3) {
+    fprintf(stderr, "usage: test <graph-prefix> <pattern.g> [--labeled=0|1] [--truncate=N] [--device=D]\n"
+                    "            [--paged] [--frame-mb=M] [--page-kb=K] [--batch=<list>]\n");
+    return 2;
+  }
+  const char* prefix = argv[1];
+  std::string pattern = argv[2];
+  int labeled = 1, truncate = 0, device = 0, paged = 0;
+  long long frame_mb = 4096, page_kb = 64;
+  std::string batch;
+  for (int i = 3; i < argc; i++) {
+    const char* a = argv[i];
+    if (!strncmp(a, "--labeled=", 10)) labeled = atoi(a + 10);
+    else if (!strncmp(a, "--truncate=", 11)) truncate = atoi(a + 11);
+    else if (!strncmp(a, "--device=", 9)) device = atoi(a + 9);
+    else if (!strcmp(a, "--paged")) paged = 1;
+    else if (!strncmp(a, "--frame-mb=", 11)) frame_mb = atoll(a + 11);
+    else if (!strncmp(a, "--page-kb=", 10)) page_kb = atoll(a + 10);
+    else if (!strncmp(a, "--batch=", 8)) batch = a + 8;
+    else { fprintf(stderr, "test: unknown option %s\n", a); return 2; }
+  }
+  std::vector<std::string> files;
+  if (batch.empty()) {
+    files.push_back(pattern);
+  } else {
+    std::ifstream f(batch);
+    if (!f.good()) { fprintf(stderr, "test: cannot open %s\n", batch.c_str()); return 1; }
+    std::string line;
+    while (std::getline(f, line))
+      if (!line.empty() && line[0] != '#') files.push_back(line);
+  }
+
+  pm_graph_opts go;
+  pm_graph_opts_default(&go);
+  go.labeled = labeled;
+  go.device = device;
+  if (paged) {
+    go.residency = PM_RESIDENT_PAGED;
+    go.frame_pool_bytes = (uint64_t)frame_mb << 20;
+    go.page_bytes = (uint32_t)(page_kb << 10);
+  }
+  pm_graph* g = nullptr;
+  pm_status s = pm_graph_open(prefix, &go, &g);
+  if (s != PM_OK) return die("graph", s);
+  pm_graph_info gi;
+  pm_graph_get_info(g, &gi);
+  fprintf(stderr, "graph: %lld vertices, %lld adjacency entries, max degree %d, device bytes %llu\n",
+          (long long)gi.n_vertices, (long long)gi.n_adj, gi.max_degree, (unsigned long long)gi.device_bytes);
+
+  std::vector<pm_plan*> plans;
+  for (auto& f : files) {
+    pm_plan* p = nullptr;
+    s = pm_plan_compile(f.c_str(), labeled, &p);
+    if (s != PM_OK) return die(f.c_str(), s);
+    plans.push_back(p);
+  }
+  pm_ctx* ctx = nullptr;
+  s = pm_ctx_create(device, &ctx);
+  if (s != PM_OK) return die("context", s);
+  pm_run_opts ro;
+  pm_run_opts_default(&ro);
+  ro.truncate = truncate;
+  std::vector<uint64_t> counts(plans.size(), 0);
+  pm_stats st;
+  s = pm_match(ctx, g, plans.data(), (int)plans.size(), &ro, counts.data(), &st);
+  if (s != PM_OK) return die("match", s);
+  fprintf(stderr, "roots %llu, set ops %llu, algorithmic bytes %llu, root filter %.3f ms\n",
+          (unsigned long long)st.n_roots, (unsigned long long)st.set_ops,
+          (unsigned long long)st.alg_bytes, st.roots_ms);
+  const float ms = st.kernel_ms;
+  for (size_t i = 0; i < plans.size(); i++) {
+    std::cout << ms << ' ' << (unsigned long long)counts[i] << std::endl;
+    FILE* out = fopen("result.txt", "a");
+    if (out) {
+      fprintf(out, "%s\t%s\t%f\t%llu\n", prefix, files[i].c_str(), ms, (unsigned long long)counts[i]);
+      fclose(out);
+    } else {
+      fprintf(stderr, "test: cannot append to result.txt\n");
+    }
+  }
+  for (auto* p : plans) pm_plan_free(p);
+  pm_ctx_destroy(ctx);
+  pm_graph_close(g);
+  return 0;
+}

@@ -1,0 +1,1002 @@
+// pm_device.cu -- device half of libpumatch_b200.so: graph placement, the GPU
+// root filter, and the persistent DFS subgraph-enumeration kernel.
+//
+// Kernel design (sm_100a, 148 SMs):
+//   * one persistent grid, sized to the SM count times the resident blocks
+//     per SM; every warp runs its own depth-first search;
+//   * work = root edges (v0, v1) of one or more plans, handed out in chunks
+//     by 64-bit atomic cursors (one per plan, warps start on different plans
+//     so a batch of patterns interleaves);
+//   * a warp that still has a large level-1 candidate range when the queue
+//     has run dry donates the upper half of that range to a global donation
+//     ring that idle warps drain (replaces the reference's disabled
+//     stealing, src/gpu_match.cu:21-148, 818-853);
+//   * each level's candidate sets ("slots") are computed by a warp-cooperative
+//     sorted-set operation -- 32 candidates per step, per-lane membership
+//     search, __ballot_sync/__popc compaction -- and stored in a per-warp
+//     arena in HBM sized to the plan's worst case, so nothing is truncated
+//     (the reference caps every set at GRAPH_DEGREE=4096; that cap is kept
+//     only as an explicit emulation switch);
+//   * the last level is counted, never materialised.
+#include <cub/cub.cuh>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <climits>
+#include <cstring>
+#include <memory>
+#include <vector>
+
+#include "pm_common.h"
+#include "pm_device.cuh"
+
+namespace pm {
+const Plan* plan_of(const pm_plan* h);
+}
+using namespace pm;
+
+#define CK(call)                                                                         \
+  do {                                                                                   \
+    cudaError_t e_ = (call);                                                             \
+    if (e_ != cudaSuccess)                                                               \
+      return fail(PM_ERR_CUDA, "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, \
+                  __LINE__);                                                             \
+  } while (0)
+
+static constexpr unsigned FULL = 0xffffffffu;
+
+// =====================================================================
+// Handles
+// =====================================================================
+
+// =====================================================================
+// Device helpers
+// =====================================================================
+
+__constant__ DPlan c_plans[PM_MAX_BATCH];
+
+__device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
+__device__ __forceinline__ unsigned lanemask_lt() {
+  unsigned m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+// First index of sorted A[0,len) whose element is >= ub: a 32-ary search,
+// one strided probe per lane per round (log32(len) rounds).
+__device__ __forceinline__ int warp_lower_bound(const int32_t* A, int len, int ub) {
+  const int lane = lane_id();
+  int lo = 0, hi = len;
+  while (hi - lo > 32) {
+    const int step = (hi - lo + 31) >> 5;
+    const long long idx = lo + (long long)lane * step;
+    const bool lt = idx < hi && A[idx] < ub;
+    const int k = __popc(__ballot_sync(FULL, lt));
+    if (k == 0) return lo;
+    const int nhi = min(hi, lo + k * step);
+    lo = lo + (k - 1) * step + 1;
+    hi = nhi;
+  }
+  const int idx = lo + lane;
+  const bool lt = idx < hi && A[idx] < ub;
+  return lo + __popc(__ballot_sync(FULL, lt));
+}
+
+// Membership of a in sorted B[0, len) by binary search (per lane).
+__device__ __forceinline__ bool bsearch_in(const int32_t* B, int len, int a) {
+  int lo = 0, hi = len;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (B[mid] < a) lo = mid + 1; else hi = mid;
+  }
+  return lo < len && B[lo] == a;
+}
+
+struct MatchArgs {
+  const uint64_t* rowptr;
+  const int32_t* colidx;
+  const uint8_t* labels;
+  int32_t n;
+  int32_t nplans;
+  int32_t T;
+  int32_t chunk;
+  int32_t shard_rank;
+  int32_t shard_count;
+  int32_t split_min;          // donate level-1 ranges at least this long
+  int32_t pad0;
+  unsigned long long* cursors;  // [nplans]
+  unsigned long long* counts;   // [nplans]
+  unsigned long long* stats;    // [8]
+  unsigned int* status;
+  int32_t* arena;
+  int64_t arena_words;          // per warp
+  unsigned long long* root_counts;
+  float* root_cost;
+  const int32_t* root_order;
+  // donation ring: items (plan, root, begin, end) -- level-1 ranges
+  int4* don_items;
+  unsigned long long* don_head;   // next slot to fill
+  unsigned long long* don_ready;  // per slot: sequence number + 1 when filled
+  unsigned int don_mask;
+  unsigned int* active;           // warps holding work (phase 1 or a donation)
+  unsigned int total_warps;
+  unsigned long long* don_tail;   // next slot to take
+  DPaging pg;
+};
+
+enum { ST_SETOPS = 0, ST_BYTES = 1, ST_ROOTS = 2, ST_SPLITS = 3 };
+
+struct WarpState {
+  int32_t path[8];
+  int32_t iter[8];
+  int32_t iend[8];   // exclusive end of the iteration range per level
+  int32_t top[9];    // arena offset where level L's slots start
+  int32_t off[16];
+  int32_t size[16];
+};
+
+// Adjacency list of v.  HBM residency: a slice of colidx.
+__device__ __forceinline__ const int32_t* adj(const MatchArgs& a, int v, int& len) {
+  const uint64_t b = a.rowptr[v];
+  len = (int)(a.rowptr[v + 1] - b);
+  return a.colidx + b;
+}
+
+// ---------------------------------------------------------------------
+// One slot of level L for the warp's current path.  Restates compute_set
+// (src/gpu_match.cu:238-319) with the operand choice of extend
+// (src/gpu_match.cu:409-812): returns the slot size (at the last level the
+// count), writes the slot to arena[top...] unless `last`.
+// ---------------------------------------------------------------------
+template <bool LABELED>
+__device__ int run_slot(const MatchArgs& a, const DPlan& P, WarpState& S, int32_t* arena, int L,
+                        int s, int top, bool last, unsigned long long& setops,
+                        unsigned long long& bytes, unsigned int& err) {
+  const int lane = lane_id();
+  const int kind = P.kind[s];
+  const int vL = S.path[L];
+  const int32_t* A;
+  const int32_t* B = nullptr;
+  int lenA, lenB = 0;
+  if (kind != SLOT_COPY) {
+    A = adj(a, vL, lenA);
+  } else if (L > 1) {
+    A = arena + S.off[P.parent[s]];
+    lenA = S.size[P.parent[s]];
+  } else {
+    A = adj(a, S.path[0], lenA);
+  }
+  if (kind == SLOT_INTERSECT) {
+    if (L > 1) {
+      B = arena + S.off[P.parent[s]];
+      lenB = S.size[P.parent[s]];
+    } else {
+      B = adj(a, S.path[0], lenB);
+    }
+  }
+
+  // symmetry-breaking upper bound (unlabeled only, src/gpu_match.cu:426-458)
+  if (!LABELED && P.partial[s]) {
+    const bool is_main = (s == P.level_begin[L]);
+    long long ub = is_main ? INT_MAX : -1;
+    for (int j = 0; j <= L; j++) {
+      if (!(P.partial[s] & (1u << j))) continue;
+      const long long v = S.path[j];
+      if (is_main) { if (v <= ub) ub = v; }
+      else if (ub < v) ub = v;
+    }
+    if (ub == -1) ub = INT_MAX;
+    if (ub != INT_MAX) lenA = warp_lower_bound(A, lenA, (int)ub);
+  }
+
+  const int T = a.T;
+  int scan = lenA;
+  const bool fresh_unl = (!LABELED && kind == SLOT_FRESH);
+  if (fresh_unl && T && scan > T) scan = T;  // first pass keeps A's prefix
+  if (!last && top + scan > a.arena_words) {
+    err |= DEV_ARENA_OVERFLOW;
+    return 0;
+  }
+  int32_t* out = arena + top;
+  const uint32_t mask = P.slot_labels[s];
+  int cnt = 0;
+  for (int base = 0; base < scan; base += 32) {
+    const int i = base + lane;
+    const bool valid = i < scan;
+    const int x = valid ? A[i] : 0;
+    bool keep = valid;
+    if (kind == SLOT_INTERSECT && keep) keep = bsearch_in(B, lenB, x);
+    if (LABELED) {
+      if (keep) keep = (mask >> a.labels[x]) & 1u;
+    } else if (kind == SLOT_COPY) {
+      keep = keep && x != vL;
+    } else if (kind == SLOT_FRESH) {
+      for (int j = 0; j <= L; j++) keep = keep && x != S.path[j];
+    }
+    const unsigned bal = __ballot_sync(FULL, keep);
+    if (!last && keep) {
+      const int pos = cnt + __popc(bal & lanemask_lt());
+      if (!T || pos < T) out[pos] = x;
+    }
+    cnt += __popc(bal);
+    if (T && cnt >= T && !fresh_unl) break;  // result is the first T survivors
+  }
+  if (T && cnt > T) cnt = T;
+  setops++;
+  bytes += 4ull * (unsigned long long)(lenA + lenB + cnt) + (LABELED ? (unsigned long long)lenA : 0ull);
+  return cnt;
+}
+
+// Computes every slot of level L; returns the arena top after them.
+template <bool LABELED>
+__device__ __forceinline__ int run_level(const MatchArgs& a, const DPlan& P, WarpState& S,
+                                         int32_t* arena, int L, unsigned long long& setops,
+                                         unsigned long long& bytes, unsigned int& err) {
+  int top = S.top[L];
+  for (int s = P.level_begin[L]; s < P.level_begin[L + 1]; s++) {
+    const int sz = run_slot<LABELED>(a, P, S, arena, L, s, top, false, setops, bytes, err);
+    if (lane_id() == 0) { S.off[s] = top; S.size[s] = sz; }
+    top += sz;
+  }
+  if (lane_id() == 0) S.top[L + 1] = top;
+  __syncwarp();
+  return top;
+}
+
+// Depth-first enumeration below a root edge, over level-1 candidates
+// [b1, e1) (e1 < 0: all).  Restates match() (src/gpu_match.cu:855-1047)
+// without deferral: every branch is finished where it starts.
+template <bool LABELED>
+__device__ unsigned long long dfs_root(const MatchArgs& a, const DPlan& P, WarpState& S,
+                                       int32_t* arena, int v0, int v1, int b1, int e1,
+                                       bool may_split, int plan_id, int root_id,
+                                       unsigned long long& setops, unsigned long long& bytes,
+                                       unsigned int& err) {
+  const int lane = lane_id();
+  const int n = P.nnodes;
+  if (lane == 0) { S.path[0] = v0; S.path[1] = v1; S.top[1] = 0; }
+  __syncwarp();
+  if (n == 3) return (unsigned long long)run_slot<LABELED>(a, P, S, arena, 1, P.level_begin[1], 0, true, setops, bytes, err);
+  run_level<LABELED>(a, P, S, arena, 1, setops, bytes, err);
+  if (err) return 0;
+  unsigned long long cnt = 0;
+  const int m1 = P.level_begin[1];
+  int end1 = S.size[m1];
+  if (e1 >= 0 && e1 < end1) end1 = e1;
+  if (lane == 0) { S.iter[1] = b1; S.iend[1] = end1; }
+  __syncwarp();
+  int L = 1;
+  while (true) {
+    const int m = P.level_begin[L];
+    int it = S.iter[L];
+    int iend = (L == 1) ? S.iend[1] : S.size[m];
+    // donate the upper half of a long level-1 range when warps are idle
+    if (L == 1 && may_split && a.split_min > 0 && iend - it >= a.split_min) {
+      int give = 0;
+      if (lane == 0) {
+        const unsigned int act = *((volatile unsigned int*)a.active);
+        const unsigned long long head = *((volatile unsigned long long*)a.don_head);
+        const unsigned long long tail = *((volatile unsigned long long*)a.don_tail);
+        // only while some warps idle and fewer ranges are queued than idle warps
+        if (act < a.total_warps && head - tail < (unsigned long long)(a.total_warps - act)) {
+          const unsigned long long slot = atomicAdd(a.don_head, 1ull);
+          const int mid = it + (iend - it) / 2;
+          a.don_items[slot & a.don_mask] = make_int4(plan_id, root_id, mid, iend);
+          __threadfence();
+          atomicExch(&a.don_ready[slot & a.don_mask], slot + 1);
+          atomicAdd(&a.stats[ST_SPLITS], 1ull);
+          give = mid;
+        }
+      }
+      give = __shfl_sync(FULL, give, 0);
+      if (give) {
+        iend = give;
+        if (lane == 0) S.iend[1] = give;
+        __syncwarp();
+      }
+    }
+    if (it < iend) {
+      const int v = arena[S.off[m] + it];
+      if (lane == 0) { S.iter[L] = it + 1; S.path[L + 1] = v; }
+      __syncwarp();
+      if (L + 1 == n - 2) {
+        cnt += (unsigned long long)run_slot<LABELED>(a, P, S, arena, L + 1, P.last_slot, S.top[L + 1], true, setops, bytes, err);
+      } else {
+        L++;
+        run_level<LABELED>(a, P, S, arena, L, setops, bytes, err);
+        if (lane == 0) S.iter[L] = 0;
+        __syncwarp();
+      }
+      if (err) return 0;
+    } else {
+      L--;
+      if (L < 1) break;
+    }
+  }
+  return cnt;
+}
+
+// Takes one donated level-1 range if any is queued.  The caller is counted
+// as active before it claims, so "no active warp and nothing queued" is a
+// safe exit test for everyone.  Returns false if nothing was taken.
+__device__ bool take_donation(const MatchArgs& a, int4& item) {
+  int got = 0;
+  int4 it = make_int4(0, 0, 0, 0);
+  if (lane_id() == 0) {
+    const unsigned long long tail = *((volatile unsigned long long*)a.don_tail);
+    const unsigned long long head = *((volatile unsigned long long*)a.don_head);
+    if (tail < head) {
+      atomicAdd(a.active, 1u);
+      __threadfence();
+      if (atomicCAS(a.don_tail, tail, tail + 1) == tail) {
+        // bounded wait for the donor to finish writing this slot
+        for (int spin = 0; spin < (1 << 22); spin++) {
+          if (*((volatile unsigned long long*)&a.don_ready[tail & a.don_mask]) == tail + 1) { got = 1; break; }
+          __nanosleep(64);
+        }
+        if (got) {
+          __threadfence();
+          const volatile int* src = (const volatile int*)&a.don_items[tail & a.don_mask];
+          it = make_int4(src[0], src[1], src[2], src[3]);
+        } else {
+          atomicOr(a.status, (unsigned)DEV_TIMEOUT);
+          atomicSub(a.active, 1u);
+        }
+      } else {
+        atomicSub(a.active, 1u);
+      }
+    }
+  }
+  got = __shfl_sync(FULL, got, 0);
+  item.x = __shfl_sync(FULL, it.x, 0);
+  item.y = __shfl_sync(FULL, it.y, 0);
+  item.z = __shfl_sync(FULL, it.z, 0);
+  item.w = __shfl_sync(FULL, it.w, 0);
+  return got != 0;
+}
+
+template <bool LABELED>
+__global__ void __launch_bounds__(256) match_kernel(MatchArgs a) {
+  extern __shared__ WarpState smem_state[];
+  const int lane = lane_id();
+  const int wib = threadIdx.x >> 5;
+  WarpState& S = smem_state[wib];
+  const long long gw = (long long)blockIdx.x * (blockDim.x >> 5) + wib;
+  int32_t* arena = a.arena + gw * a.arena_words;
+  unsigned long long setops = 0, bytes = 0, roots = 0;
+  unsigned int err = 0;
+  const int np = a.nplans;
+  int p = (int)(gw % np);
+  int exhausted = 0;
+  // phase 1: root chunks from the per-plan cursors
+  while (exhausted < np && !err) {
+    const DPlan& P = c_plans[p];
+    const unsigned long long nchunks = (unsigned long long)((P.nroots + a.chunk - 1) / a.chunk);
+    unsigned long long c = 0;
+    if (lane == 0) c = atomicAdd(&a.cursors[p], 1ull);
+    c = __shfl_sync(FULL, c, 0);
+    const unsigned long long gc = c * (unsigned long long)a.shard_count + (unsigned long long)a.shard_rank;
+    if (gc >= nchunks) {
+      exhausted++;
+      p = (p + 1 == np) ? 0 : p + 1;
+      continue;
+    }
+    exhausted = 0;
+    const long long rb = (long long)gc * a.chunk;
+    const long long re = min((long long)P.nroots, rb + a.chunk);
+    unsigned long long local = 0;
+    for (long long r = rb; r < re && !err; r++) {
+      const long long rid = a.root_order ? (long long)a.root_order[r] : r;
+      const int2 e = P.roots[rid];
+      const unsigned long long b0 = bytes;
+      const unsigned long long c0 = LABELED
+          ? dfs_root<true>(a, P, S, arena, e.x, e.y, 0, -1, true, p, (int)rid, setops, bytes, err)
+          : dfs_root<false>(a, P, S, arena, e.x, e.y, 0, -1, true, p, (int)rid, setops, bytes, err);
+      local += c0;
+      roots++;
+      if (lane == 0 && p == 0) {
+        if (a.root_counts) atomicAdd(&a.root_counts[rid], c0);
+        if (a.root_cost) atomicAdd(&a.root_cost[rid], (float)(bytes - b0 + 8));
+      }
+    }
+    if (lane == 0 && local) atomicAdd(&a.counts[p], local);
+    p = (p + 1 == np) ? 0 : p + 1;  // interleave plans chunk by chunk
+  }
+  // phase 2: drain donated level-1 ranges until no warp holds work
+  __threadfence();
+  if (lane == 0) atomicSub(a.active, 1u);
+  __syncwarp();
+  for (long long idle_spins = 0; !err;) {
+    int4 item;
+    if (take_donation(a, item)) {
+      const DPlan& P = c_plans[item.x];
+      const int2 e = P.roots[item.y];
+      const unsigned long long b0 = bytes;
+      const unsigned long long c0 = LABELED
+          ? dfs_root<true>(a, P, S, arena, e.x, e.y, item.z, item.w, true, item.x, item.y, setops, bytes, err)
+          : dfs_root<false>(a, P, S, arena, e.x, e.y, item.z, item.w, true, item.x, item.y, setops, bytes, err);
+      if (lane == 0) {
+        if (c0) atomicAdd(&a.counts[item.x], c0);
+        if (item.x == 0) {
+          if (a.root_counts) atomicAdd(&a.root_counts[item.y], c0);
+          if (a.root_cost) atomicAdd(&a.root_cost[item.y], (float)(bytes - b0));
+        }
+        __threadfence();
+        atomicSub(a.active, 1u);
+      }
+      __syncwarp();
+      idle_spins = 0;
+      continue;
+    }
+    unsigned int act = 0;
+    unsigned long long head = 0, tail = 0;
+    if (lane == 0) {
+      act = *((volatile unsigned int*)a.active);
+      __threadfence();
+      head = *((volatile unsigned long long*)a.don_head);
+      tail = *((volatile unsigned long long*)a.don_tail);
+    }
+    act = __shfl_sync(FULL, act, 0);
+    head = __shfl_sync(FULL, head, 0);
+    tail = __shfl_sync(FULL, tail, 0);
+    if (act == 0 && tail >= head) break;
+    if (++idle_spins > (1ll << 28)) {  // bounded polling; the host sees DEV_TIMEOUT
+      if (lane == 0) atomicOr(a.status, (unsigned)DEV_TIMEOUT);
+      break;
+    }
+    __nanosleep(256);
+  }
+  if (lane == 0) {
+    atomicAdd(&a.stats[ST_SETOPS], setops);
+    atomicAdd(&a.stats[ST_BYTES], bytes + 8ull * roots);
+    atomicAdd(&a.stats[ST_ROOTS], roots);
+    if (err) atomicOr(a.status, err);
+  }
+}
+
+// =====================================================================
+// Root filter (restates JobQueuePreprocessor, src/job_queue.h:39-64, as
+// three passes: per-vertex max neighbour degree, per-vertex root counts +
+// scan, ordered write).  Root order = reference order (r ascending, then
+// adjacency order), so root ids match the reference's Job[] indices.
+// =====================================================================
+
+__global__ void maxnbrdeg_kernel(const uint64_t* rowptr, const int32_t* colidx, int64_t n, int32_t* out) {
+  const int lane = lane_id();
+  const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
+  for (long long v = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); v < n; v += warps) {
+    const uint64_t b = rowptr[v], e = rowptr[v + 1];
+    int m = 0;
+    for (uint64_t i = b + lane; i < e; i += 32) {
+      const int u = colidx[i];
+      m = max(m, (int)(rowptr[u + 1] - rowptr[u]));
+    }
+    for (int o = 16; o; o >>= 1) m = max(m, __shfl_xor_sync(FULL, m, o));
+    if (lane == 0) out[v] = m;
+  }
+}
+
+struct RootFilter {
+  int labeled;
+  int need_gt;   // unlabeled with partial[0]==1: keep r > c only
+  int lab0, lab1;
+  int d0, d1, d2;
+};
+
+template <bool WRITE>
+__global__ void roots_kernel(const uint64_t* rowptr, const int32_t* colidx, const uint8_t* labels,
+                             const int32_t* maxnbrdeg, int64_t n, RootFilter f, int32_t* counts,
+                             const int64_t* offsets, int2* out) {
+  const int lane = lane_id();
+  const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
+  for (long long r = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); r < n; r += warps) {
+    const uint64_t b = rowptr[r], e = rowptr[r + 1];
+    int total = 0;
+    const bool rok = (long long)(e - b) >= f.d0 && (!f.labeled || labels[r] == f.lab0);
+    if (rok) {
+      long long base = WRITE ? offsets[r] : 0;
+      for (uint64_t i0 = b; i0 < e; i0 += 32) {
+        const uint64_t i = i0 + lane;
+        bool keep = false;
+        if (i < e) {
+          const int c = colidx[i];
+          keep = (!f.need_gt || r > c) && (!f.labeled || labels[c] == f.lab1) &&
+                 (int)(rowptr[c + 1] - rowptr[c]) >= f.d1 && maxnbrdeg[c] >= f.d2;
+        }
+        const unsigned bal = __ballot_sync(FULL, keep);
+        if (WRITE && keep) out[base + total + __popc(bal & lanemask_lt())] = make_int2((int)r, colidx[i]);
+        total += __popc(bal);
+      }
+    }
+    if (!WRITE && lane == 0) counts[r] = total;
+  }
+}
+
+// =====================================================================
+// Host glue
+// =====================================================================
+
+namespace {
+
+void free_dev(void* p) { if (p) cudaFree(p); }
+
+pm_status ensure(void** p, size_t* have, size_t want) {
+  if (*have >= want && *p) return PM_OK;
+  free_dev(*p);
+  *p = nullptr;
+  *have = 0;
+  if (want == 0) return PM_OK;
+  cudaError_t e = cudaMalloc(p, want);
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    return fail(PM_ERR_OOM, "cudaMalloc(%zu) failed: %s", want, cudaGetErrorString(e));
+  }
+  *have = want;
+  return PM_OK;
+}
+
+pm_status check_device(int device) {
+  int count = 0;
+  cudaError_t e = cudaGetDeviceCount(&count);
+  if (e != cudaSuccess || count == 0)
+    return fail(PM_ERR_NO_DEVICE, "no CUDA device available (%s); libpumatch_b200 has no CPU path",
+                e == cudaSuccess ? "0 devices" : cudaGetErrorString(e));
+  if (device < 0 || device >= count) return fail(PM_ERR_INVALID, "device %d out of range", device);
+  CK(cudaSetDevice(device));
+  return PM_OK;
+}
+
+DPlan to_dplan(const Plan& p) {
+  DPlan d;
+  memset(&d, 0, sizeof(d));
+  d.nnodes = p.nnodes;
+  d.nslots = p.nslots;
+  d.labeled = p.labeled;
+  d.last_slot = p.level_begin[p.nnodes - 2];
+  for (int i = 0; i <= PM_MAX_PAT; i++) d.level_begin[i] = p.level_begin[i];
+  for (int s = 0; s < p.nslots; s++) {
+    d.slot_labels[s] = p.slot_labels[s];
+    d.partial[s] = p.partial[s];
+    d.kind[s] = (uint8_t)slot_kind(p.set_ops[s]);
+    d.parent[s] = (uint8_t)slot_parent(p.set_ops[s]);
+  }
+  return d;
+}
+
+RootFilter to_filter(const Plan& p) {
+  RootFilter f;
+  f.labeled = p.labeled;
+  f.need_gt = (!p.labeled && p.partial[0] == 1);
+  f.lab0 = p.vertex_label[0];
+  f.lab1 = p.vertex_label[1];
+  f.d0 = p.degree[0];
+  f.d1 = p.degree[1];
+  f.d2 = p.degree[2];
+  return f;
+}
+
+// Worst-case arena words one warp needs for a plan: every materialised slot
+// is at most its first operand, itself at most a max-degree list.
+int64_t arena_words_for(const Plan& p, int32_t maxdeg, int T) {
+  const int64_t per = (T > 0) ? std::min<int64_t>(maxdeg, T) : maxdeg;
+  const int materialised = p.nslots - 2;  // minus the root slot and the counted last slot
+  return std::max<int64_t>(materialised, 1) * per + 64;
+}
+
+}  // namespace
+
+static pm_status graph_finish(pm_graph* g) {
+  // per-vertex max neighbour degree, used by the root filter
+  CK(cudaMalloc(&g->d_maxnbrdeg, sizeof(int32_t) * std::max<int64_t>(g->n, 1)));
+  g->device_bytes += sizeof(int32_t) * g->n;
+  if (g->n > 0 && g->residency == PM_RESIDENT_HBM) {
+    maxnbrdeg_kernel<<<2048, 256>>>(g->d_rowptr, g->d_colidx, g->n, g->d_maxnbrdeg);
+    CK(cudaGetLastError());
+    CK(cudaDeviceSynchronize());
+  }
+  return PM_OK;
+}
+
+namespace pm {
+pm_status paged_place(pm_graph* g, const int32_t* colidx, const pm_graph_opts* o);
+pm_status paged_maxnbrdeg(pm_graph* g);
+void paged_release(pm_graph* g);
+pm_status paged_prepare(pm_ctx* ctx, pm_graph* g, DPaging* out);
+pm_status paged_service_start(pm_ctx* ctx, pm_graph* g, const DPaging& pg);
+pm_status paged_service_stop(pm_ctx* ctx, pm_graph* g, pm_stats* st);
+}  // namespace pm
+
+extern "C" void pm_graph_opts_default(pm_graph_opts* o) {
+  if (!o) return;
+  memset(o, 0, sizeof(*o));
+  o->labeled = 0;
+  o->device = 0;
+  o->residency = PM_RESIDENT_HBM;
+  o->page_bytes = 64 * 1024;
+  o->frame_pool_bytes = 4ull << 30;
+}
+
+extern "C" pm_status pm_graph_from_host(int64_t n, int64_t nadj, const uint64_t* rowptr, const int32_t* colidx,
+                                        const uint32_t* labels, const pm_graph_opts* opts, pm_graph** out) {
+  if (!rowptr || (nadj > 0 && !colidx) || !out || n < 0 || n > INT32_MAX - 1)
+    return fail(PM_ERR_INVALID, "pm_graph_from_host: bad arguments");
+  pm_graph_opts o;
+  pm_graph_opts_default(&o);
+  if (opts) o = *opts;
+  pm_status st = check_device(o.device);
+  if (st != PM_OK) return st;
+  if (o.labeled && !labels) return fail(PM_ERR_INVALID, "labeled graph without labels");
+  std::unique_ptr<pm_graph> g(new pm_graph);
+  g->device = o.device;
+  g->n = n;
+  g->nadj = nadj;
+  g->labeled = o.labeled ? 1 : 0;
+  g->residency = o.residency;
+  int32_t maxd = 0;
+  for (int64_t v = 0; v < n; v++) maxd = std::max<int32_t>(maxd, (int32_t)(rowptr[v + 1] - rowptr[v]));
+  g->maxdeg = maxd;
+  CK(cudaMalloc(&g->d_rowptr, sizeof(uint64_t) * (n + 1)));
+  CK(cudaMemcpy(g->d_rowptr, rowptr, sizeof(uint64_t) * (n + 1), cudaMemcpyHostToDevice));
+  g->device_bytes += sizeof(uint64_t) * (n + 1);
+  if (g->labeled) {
+    std::vector<uint8_t> lab((size_t)std::max<int64_t>(n, 1));
+    int nl = 0;
+    for (int64_t v = 0; v < n; v++) {
+      if (labels[v] >= 32) return fail(PM_ERR_FORMAT, "label %u of vertex %lld >= 32", labels[v], (long long)v);
+      lab[v] = (uint8_t)labels[v];
+      nl = std::max<int>(nl, (int)labels[v] + 1);
+    }
+    g->nlabels = nl;
+    CK(cudaMalloc(&g->d_labels, std::max<int64_t>(n, 1)));
+    CK(cudaMemcpy(g->d_labels, lab.data(), n, cudaMemcpyHostToDevice));
+    g->device_bytes += n;
+  }
+  if (o.residency == PM_RESIDENT_PAGED) {
+    st = paged_place(g.get(), colidx, &o);
+    if (st != PM_OK) return st;
+    CK(cudaMalloc(&g->d_maxnbrdeg, sizeof(int32_t) * std::max<int64_t>(g->n, 1)));
+    g->device_bytes += sizeof(int32_t) * g->n;
+    st = paged_maxnbrdeg(g.get());
+    if (st != PM_OK) return st;
+  } else {
+    CK(cudaMalloc(&g->d_colidx, sizeof(int32_t) * std::max<int64_t>(nadj, 1)));
+    if (nadj) CK(cudaMemcpy(g->d_colidx, colidx, sizeof(int32_t) * nadj, cudaMemcpyHostToDevice));
+    g->device_bytes += sizeof(int32_t) * nadj;
+    st = graph_finish(g.get());
+    if (st != PM_OK) return st;
+  }
+  *out = g.release();
+  return PM_OK;
+}
+
+extern "C" pm_status pm_graph_from_device(int64_t n, int64_t nadj, int32_t maxdeg, const uint64_t* d_rowptr,
+                                          const int32_t* d_colidx, const uint8_t* d_labels, int device,
+                                          pm_graph** out) {
+  if (!d_rowptr || (nadj > 0 && !d_colidx) || !out || n < 0 || maxdeg < 0)
+    return fail(PM_ERR_INVALID, "pm_graph_from_device: bad arguments");
+  pm_status st = check_device(device);
+  if (st != PM_OK) return st;
+  std::unique_ptr<pm_graph> g(new pm_graph);
+  g->device = device;
+  g->n = n;
+  g->nadj = nadj;
+  g->maxdeg = maxdeg;
+  g->labeled = d_labels != nullptr;
+  g->nlabels = d_labels ? 32 : 0;
+  g->owns = false;
+  g->d_rowptr = const_cast<uint64_t*>(d_rowptr);
+  g->d_colidx = const_cast<int32_t*>(d_colidx);
+  g->d_labels = const_cast<uint8_t*>(d_labels);
+  st = graph_finish(g.get());
+  if (st != PM_OK) return st;
+  *out = g.release();
+  return PM_OK;
+}
+
+extern "C" pm_status pm_graph_open(const char* prefix, const pm_graph_opts* opts, pm_graph** out) {
+  pm_graph_opts o;
+  pm_graph_opts_default(&o);
+  if (opts) o = *opts;
+  int64_t n = 0, nadj = 0;
+  int32_t maxd = 0;
+  uint64_t* rowptr = nullptr;
+  int32_t* colidx = nullptr;
+  uint32_t* labels = nullptr;
+  pm_status st = pm_graph_read(prefix, o.labeled, &n, &nadj, &maxd, &rowptr, &colidx, &labels);
+  if (st != PM_OK) return st;
+  st = pm_graph_from_host(n, nadj, rowptr, colidx, labels, &o, out);
+  free(rowptr);
+  free(colidx);
+  free(labels);
+  return st;
+}
+
+extern "C" pm_status pm_graph_get_info(const pm_graph* g, pm_graph_info* info) {
+  if (!g || !info) return fail(PM_ERR_INVALID, "pm_graph_get_info: null argument");
+  memset(info, 0, sizeof(*info));
+  info->n_vertices = g->n;
+  info->n_adj = g->nadj;
+  info->max_degree = g->maxdeg;
+  info->labeled = g->labeled;
+  info->n_labels = g->nlabels;
+  info->residency = g->residency;
+  info->device_bytes = g->device_bytes;
+  info->n_pages = (uint64_t)g->n_pages;
+  info->n_frames = (uint64_t)g->n_frames;
+  return PM_OK;
+}
+
+extern "C" void pm_graph_close(pm_graph* g) {
+  if (!g) return;
+  cudaSetDevice(g->device);
+  if (g->owns) {
+    free_dev(g->d_rowptr);
+    free_dev(g->d_colidx);
+    free_dev(g->d_labels);
+  }
+  free_dev(g->d_maxnbrdeg);
+  paged_release(g);
+  delete g;
+}
+
+extern "C" pm_status pm_ctx_create(int device, pm_ctx** out) {
+  if (!out) return fail(PM_ERR_INVALID, "pm_ctx_create: null argument");
+  pm_status st = check_device(device);
+  if (st != PM_OK) return st;
+  std::unique_ptr<pm_ctx> c(new pm_ctx);
+  c->device = device;
+  CK(cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, device));
+  CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+  CK(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
+  for (auto& e : c->ev) CK(cudaEventCreate(&e));
+  *out = c.release();
+  return PM_OK;
+}
+
+extern "C" void pm_ctx_destroy(pm_ctx* c) {
+  if (!c) return;
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  cudaStreamSynchronize(c->copy_stream);
+  free_dev(c->d_arena);
+  free_dev(c->d_ctl);
+  free_dev(c->d_roots);
+  free_dev(c->d_tmp);
+  free_dev(c->d_vcount);
+  free_dev(c->d_voff);
+  for (auto& e : c->ev) if (e) cudaEventDestroy(e);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
+  delete c;
+}
+
+extern "C" void pm_run_opts_default(pm_run_opts* o) {
+  if (!o) return;
+  memset(o, 0, sizeof(*o));
+  o->root_begin = -1;
+  o->root_end = -1;
+}
+
+// Builds the root list of plan p into ctx->d_roots + offset; returns count.
+static pm_status build_roots(pm_ctx* c, const pm_graph* g, const Plan& p, size_t offset_roots,
+                             int64_t* count, bool count_only) {
+  const int64_t n = g->n;
+  if (n == 0) { *count = 0; return PM_OK; }
+  if (c->vbuf_n < (size_t)n + 1) {
+    free_dev(c->d_vcount);
+    free_dev(c->d_voff);
+    c->d_vcount = nullptr;
+    c->d_voff = nullptr;
+    c->vbuf_n = 0;
+    CK(cudaMalloc(&c->d_vcount, sizeof(int32_t) * (n + 1)));
+    CK(cudaMalloc(&c->d_voff, sizeof(int64_t) * (n + 1)));
+    c->vbuf_n = (size_t)n + 1;
+  }
+  const RootFilter f = to_filter(p);
+  const int32_t* colidx = g->residency == PM_RESIDENT_HBM ? g->d_colidx : g->h_colidx_dev;
+  roots_kernel<false><<<4 * c->nsm, 256, 0, c->stream>>>(g->d_rowptr, colidx, g->d_labels, g->d_maxnbrdeg, n, f,
+                                                          c->d_vcount, nullptr, nullptr);
+  CK(cudaGetLastError());
+  CK(cudaMemsetAsync(c->d_vcount + n, 0, sizeof(int32_t), c->stream));
+  size_t need = 0;
+  CK(cub::DeviceScan::ExclusiveSum(nullptr, need, c->d_vcount, c->d_voff, n + 1, c->stream));
+  pm_status st = ensure(&c->d_tmp, &c->tmp_bytes, need);
+  if (st != PM_OK) return st;
+  CK(cub::DeviceScan::ExclusiveSum(c->d_tmp, need, c->d_vcount, c->d_voff, n + 1, c->stream));
+  int64_t total = 0;
+  CK(cudaMemcpyAsync(&total, c->d_voff + n, sizeof(int64_t), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  *count = total;
+  if (count_only) return PM_OK;
+  const size_t want = sizeof(int2) * (offset_roots + (size_t)total);
+  if (c->roots_bytes < want) {
+    // grow, keeping the roots of earlier plans
+    int2* nr = nullptr;
+    CK(cudaMalloc(&nr, want + want / 4));
+    if (c->d_roots && offset_roots)
+      CK(cudaMemcpyAsync(nr, c->d_roots, sizeof(int2) * offset_roots, cudaMemcpyDeviceToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    free_dev(c->d_roots);
+    c->d_roots = nr;
+    c->roots_bytes = want + want / 4;
+  }
+  roots_kernel<true><<<4 * c->nsm, 256, 0, c->stream>>>(g->d_rowptr, colidx, g->d_labels, g->d_maxnbrdeg, n, f,
+                                                         nullptr, c->d_voff, c->d_roots + offset_roots);
+  CK(cudaGetLastError());
+  return PM_OK;
+}
+
+extern "C" pm_status pm_count_roots(pm_ctx* c, const pm_graph* g, const pm_plan* ph, int64_t* n_roots) {
+  if (!c || !g || !ph || !n_roots) return fail(PM_ERR_INVALID, "pm_count_roots: null argument");
+  const Plan& p = *plan_of(ph);
+  if (p.labeled && !g->labeled) return fail(PM_ERR_INVALID, "labeled plan on an unlabeled graph");
+  CK(cudaSetDevice(c->device));
+  return build_roots(c, g, p, 0, n_roots, true);
+}
+
+namespace pm {
+// Exposed for tests through pm_debug_roots: copies the root list of one plan.
+pm_status debug_roots(pm_ctx* c, const pm_graph* g, const Plan& p, int32_t* out_pairs, int64_t cap, int64_t* count) {
+  pm_status st = build_roots(c, g, p, 0, count, false);
+  if (st != PM_OK) return st;
+  const int64_t m = std::min<int64_t>(cap, *count);
+  if (m > 0) CK(cudaMemcpyAsync(out_pairs, c->d_roots, sizeof(int2) * m, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return PM_OK;
+}
+}  // namespace pm
+
+extern "C" pm_status pm_debug_roots(pm_ctx* c, const pm_graph* g, const pm_plan* ph, int32_t* out_pairs,
+                                    int64_t cap, int64_t* count) {
+  if (!c || !g || !ph || !count) return fail(PM_ERR_INVALID, "pm_debug_roots: null argument");
+  CK(cudaSetDevice(c->device));
+  return debug_roots(c, g, *plan_of(ph), out_pairs, cap, count);
+}
+
+extern "C" pm_status pm_match(pm_ctx* c, const pm_graph* g, const pm_plan* const* plans, int nplans,
+                              const pm_run_opts* opts, uint64_t* counts_out, pm_stats* stats_out) {
+  if (!c || !g || !plans || nplans < 1 || !counts_out) return fail(PM_ERR_INVALID, "pm_match: bad arguments");
+  if (nplans > PM_MAX_BATCH) return fail(PM_ERR_INVALID, "pm_match: at most %d plans per launch", PM_MAX_BATCH);
+  pm_run_opts o;
+  pm_run_opts_default(&o);
+  if (opts) o = *opts;
+  CK(cudaSetDevice(c->device));
+  const bool labeled = plan_of(plans[0])->labeled != 0;
+  for (int i = 0; i < nplans; i++) {
+    const Plan* p = plan_of(plans[i]);
+    if (!p) return fail(PM_ERR_INVALID, "pm_match: null plan %d", i);
+    if ((p->labeled != 0) != labeled) return fail(PM_ERR_INVALID, "pm_match: plans mix labeled and unlabeled modes");
+    if (p->labeled && !g->labeled) return fail(PM_ERR_INVALID, "labeled plan on an unlabeled graph");
+  }
+  if (o.root_order && nplans != 1) return fail(PM_ERR_INVALID, "root_order needs a single plan");
+  const int T = std::max(0, o.truncate);
+  const int wpb = o.warps_per_block > 0 ? o.warps_per_block : 8;
+  if (wpb > 8 || (wpb & (wpb - 1))) return fail(PM_ERR_INVALID, "warps_per_block must be 1,2,4 or 8");
+  const int chunk = o.chunk > 0 ? o.chunk : 16;
+  const int shard_count = o.shard_count > 1 ? o.shard_count : 1;
+  if (o.shard_rank < 0 || o.shard_rank >= shard_count) return fail(PM_ERR_INVALID, "bad shard_rank");
+
+  cudaEvent_t e0 = c->ev[0], e1 = c->ev[1], e2 = c->ev[2];
+  CK(cudaEventRecord(e0, c->stream));
+
+  // root lists, concatenated
+  DPlan dp[PM_MAX_BATCH];
+  size_t off = 0;
+  int64_t arena_words = 64;
+  for (int i = 0; i < nplans; i++) {
+    const Plan& p = *plan_of(plans[i]);
+    int64_t cnt = 0;
+    pm_status st = build_roots(c, g, p, off, &cnt, false);
+    if (st != PM_OK) return st;
+    dp[i] = to_dplan(p);
+    dp[i].nroots = cnt;
+    arena_words = std::max(arena_words, arena_words_for(p, g->maxdeg, T));
+    off += (size_t)cnt;
+  }
+  off = 0;
+  for (int i = 0; i < nplans; i++) {
+    int64_t b = 0, e = dp[i].nroots;
+    if (o.root_begin >= 0) b = std::min<int64_t>(o.root_begin, e);
+    if (o.root_end >= 0) e = std::min<int64_t>(o.root_end, e);
+    if (e < b) e = b;
+    dp[i].roots = c->d_roots + off + b;
+    off += (size_t)dp[i].nroots;
+    dp[i].nroots = e - b;
+  }
+  CK(cudaMemcpyToSymbolAsync(c_plans, dp, sizeof(DPlan) * nplans, 0, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaEventRecord(e1, c->stream));
+
+  // launch geometry: persistent, occupancy-limited
+  const int threads = wpb * 32;
+  const size_t smem = sizeof(WarpState) * wpb;
+  int per_sm = 0;
+  if (labeled) CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, match_kernel<true>, threads, smem));
+  else CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, match_kernel<false>, threads, smem));
+  if (o.blocks_per_sm > 0) per_sm = std::min(per_sm, o.blocks_per_sm);
+  per_sm = std::max(per_sm, 1);
+  int blocks = c->nsm * per_sm;
+  int64_t warps = (int64_t)blocks * wpb;
+  // cap the arena to half of free memory by reducing resident warps
+  size_t free_b = 0, total_b = 0;
+  CK(cudaMemGetInfo(&free_b, &total_b));
+  while (blocks > c->nsm && (size_t)(warps * arena_words * 4) > free_b / 2) {
+    blocks -= c->nsm;
+    warps = (int64_t)blocks * wpb;
+  }
+  pm_status st = ensure((void**)&c->d_arena, &c->arena_bytes, (size_t)(warps * arena_words * 4));
+  if (st != PM_OK) return st;
+
+  // control block: cursors[32] counts[32] stats[8] status idle head tail ring...
+  const unsigned don_slots = 1u << 16;
+  const size_t ctl_words = 32 + 32 + 8 + 4 + 2 * don_slots + don_slots * 2;
+  st = ensure((void**)&c->d_ctl, &c->ctl_bytes, ctl_words * 8);
+  if (st != PM_OK) return st;
+  CK(cudaMemsetAsync(c->d_ctl, 0, ctl_words * 8, c->stream));
+  MatchArgs a;
+  memset(&a, 0, sizeof(a));
+  a.rowptr = g->d_rowptr;
+  a.colidx = g->d_colidx;
+  a.labels = g->d_labels;
+  a.n = (int32_t)g->n;
+  a.nplans = nplans;
+  a.T = T;
+  a.chunk = chunk;
+  a.shard_rank = o.shard_rank;
+  a.shard_count = shard_count;
+  a.split_min = o.split_level1 == 0 ? 64 : (o.split_level1 < 0 ? 0 : o.split_level1);
+  unsigned long long* w = c->d_ctl;
+  a.cursors = w; w += 32;
+  a.counts = w; w += 32;
+  a.stats = w; w += 8;
+  a.status = (unsigned int*)w;
+  a.active = (unsigned int*)w + 1; w += 1;
+  a.don_head = w; w += 1;
+  a.don_tail = w; w += 2;
+  a.don_ready = w; w += don_slots;
+  a.don_items = (int4*)w; w += 2 * don_slots;
+  a.don_mask = don_slots - 1;
+  a.total_warps = (unsigned int)warps;
+  a.arena = c->d_arena;
+  a.arena_words = arena_words;
+  a.root_counts = (unsigned long long*)o.root_counts;
+  a.root_cost = o.root_cost;
+  a.root_order = o.root_order;
+  if (g->residency == PM_RESIDENT_PAGED) return fail(PM_ERR_INVALID, "paged residency is not available in this build");
+
+  // every warp starts active (it holds root chunks until the cursors run dry)
+  c->h_active = (unsigned int)warps;
+  CK(cudaMemcpyAsync(a.active, &c->h_active, sizeof(unsigned int), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaEventRecord(e1, c->stream));
+  if (labeled) match_kernel<true><<<blocks, threads, smem, c->stream>>>(a);
+  else match_kernel<false><<<blocks, threads, smem, c->stream>>>(a);
+  CK(cudaGetLastError());
+  CK(cudaEventRecord(e2, c->stream));
+  unsigned long long host_ctl[32 + 32 + 8 + 1];
+  CK(cudaMemcpyAsync(host_ctl, c->d_ctl, sizeof(host_ctl), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  const unsigned int status = (unsigned int)(host_ctl[72] & 0xffffffffu);
+  for (int i = 0; i < nplans; i++) {
+    const Plan& p = *plan_of(plans[i]);
+    counts_out[i] = host_ctl[32 + i] * (p.labeled ? 1ull : (uint64_t)p.multiplicity);
+  }
+  if (stats_out) {
+    memset(stats_out, 0, sizeof(*stats_out));
+    stats_out->set_ops = host_ctl[64 + ST_SETOPS];
+    stats_out->alg_bytes = host_ctl[64 + ST_BYTES];
+    stats_out->n_roots = host_ctl[64 + ST_ROOTS];
+    stats_out->splits = host_ctl[64 + ST_SPLITS];
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, e1, e2));
+    stats_out->kernel_ms = ms;
+    CK(cudaEventElapsedTime(&ms, e0, e1));
+    stats_out->roots_ms = ms;
+    stats_out->grid_blocks = blocks;
+    stats_out->block_threads = threads;
+    stats_out->arena_bytes = (uint64_t)(warps * arena_words * 4);
+    stats_out->device_status = status;
+  }
+  if (status & DEV_ARENA_OVERFLOW) return fail(PM_ERR_INTERNAL, "device: candidate set exceeded the warp arena");
+  if (status & DEV_TIMEOUT) return fail(PM_ERR_TIMEOUT, "device: a bounded wait gave up");
+  if (status) return fail(PM_ERR_INTERNAL, "device status 0x%x", status);
+  return PM_OK;
+}

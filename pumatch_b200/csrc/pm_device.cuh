@@ -1,0 +1,109 @@
+// pm_device.cuh -- device-side structures shared by the CUDA translation units
+// of libpumatch_b200.so (matching kernel, root filter, page cache).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "pm_common.h"
+
+#define PM_MAX_BATCH 32  // plans per persistent launch
+
+namespace pm {
+
+// Device status flags (pm_stats.device_status).
+enum : uint32_t {
+  DEV_ARENA_OVERFLOW = 1u << 0,  // a slot did not fit the warp's arena
+  DEV_TIMEOUT = 1u << 1,         // a bounded wait gave up
+  DEV_BAD_ROOT = 1u << 2,        // root id out of range
+};
+
+// One plan as the kernel reads it (constant memory).
+struct DPlan {
+  int32_t nnodes;
+  int32_t nslots;
+  int32_t labeled;
+  int32_t last_slot;              // the single slot of level nnodes-2
+  int32_t level_begin[PM_MAX_PAT + 1];
+  uint32_t slot_labels[16];
+  uint32_t partial[16];
+  uint8_t kind[16];               // SlotKind
+  uint8_t parent[16];
+  const int2* roots;              // (v0, v1) root edges, reference order
+  int64_t nroots;
+};
+
+// Page cache of the adjacency array (paged residency).  A page is a fixed
+// range of colidx; frames are page-sized slots of a device pool.
+struct DPaging {
+  int32_t enabled;
+  int32_t page_shift;             // log2(ints per page)
+  int64_t n_pages;
+  int64_t n_frames;
+  int32_t* page_frame;            // [n_pages]: frame, or PAGE_ABSENT / PAGE_LOADING
+  int32_t* frame_page;            // [n_frames]: page held, -1 free
+  int32_t* frame_pin;             // [n_frames]: readers in flight
+  uint8_t* frame_ref;             // [n_frames]: CLOCK reference bits
+  int32_t* frames;                // [n_frames << page_shift]
+  const int32_t* host_colidx;     // device-visible pointer to pinned host colidx
+  unsigned long long* clock_hand;
+  // fault ring in mapped pinned host memory: (page, frame) requests
+  int2* ring;                     // device-visible pointer
+  unsigned int ring_mask;
+  unsigned int* ring_head;        // device counter (slots claimed)
+  volatile unsigned int* ring_published; // host-visible: per slot sequence
+  unsigned long long* counters;   // [hits, misses, zero_copy_bytes, loads, evictions]
+};
+
+enum : int32_t { PAGE_ABSENT = -1, PAGE_LOADING = -2 };
+
+}  // namespace pm
+
+// Opaque handles of the C-ABI (pumatch.h), shared by the device TUs.
+struct pm_graph {
+  int device = 0;
+  int64_t n = 0, nadj = 0;
+  int32_t maxdeg = 0;
+  int labeled = 0;
+  int nlabels = 0;
+  int residency = PM_RESIDENT_HBM;
+  bool owns = true;
+  uint64_t* d_rowptr = nullptr;
+  int32_t* d_colidx = nullptr;   // HBM residency only
+  uint8_t* d_labels = nullptr;
+  int32_t* d_maxnbrdeg = nullptr;
+  uint64_t device_bytes = 0;
+  // paged residency
+  int32_t* h_colidx = nullptr;   // pinned, mapped
+  int32_t* h_colidx_dev = nullptr;
+  uint32_t page_ints = 0;
+  int64_t n_pages = 0, n_frames = 0;
+  int32_t* d_frames = nullptr;
+  int32_t* d_page_frame = nullptr;
+  int32_t* d_frame_page = nullptr;
+  int32_t* d_frame_pin = nullptr;
+  uint8_t* d_frame_ref = nullptr;
+};
+
+struct pm_ctx {
+  int device = 0;
+  int nsm = 0;
+  cudaStream_t stream = nullptr;
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  // reusable device scratch
+  int32_t* d_arena = nullptr;
+  size_t arena_bytes = 0;
+  unsigned long long* d_ctl = nullptr;  // cursors, counts, stats, status, donation ring
+  size_t ctl_bytes = 0;
+  int2* d_roots = nullptr;
+  size_t roots_bytes = 0;
+  void* d_tmp = nullptr;
+  size_t tmp_bytes = 0;
+  int32_t* d_vcount = nullptr;
+  int64_t* d_voff = nullptr;
+  size_t vbuf_n = 0;
+  unsigned int h_active = 0;  // staging for the initial active-warp count
+};
+

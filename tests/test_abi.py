@@ -1,0 +1,94 @@
+"""The C-ABI boundary: the library loads, exports every entry point that
+include/pumatch.h declares, the ctypes mirror matches the C struct layouts,
+and the product refuses to run without a GPU (no CPU fallback)."""
+import os
+import re
+import subprocess
+
+import pytest
+import torch
+
+import pumatch_b200 as pm
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADERS = [os.path.join(ROOT, "include", f) for f in os.listdir(os.path.join(ROOT, "include")) if f.endswith(".h")]
+
+
+def declared():
+    names = set()
+    for h in HEADERS:
+        src = re.sub(r"/\*.*?\*/", "", open(h).read(), flags=re.S)
+        names |= set(re.findall(r"^[A-Za-z_][\w \*]*?\b(pm_\w+)\s*\(", src, flags=re.M))
+    return names
+
+
+def test_header_declares_entry_points():
+    names = declared()
+    for n in ("pm_graph_open", "pm_plan_compile", "pm_match", "pm_ctx_create", "pm_strerror"):
+        assert n in names
+
+
+def test_library_exports_every_declared_symbol():
+    out = subprocess.run(["nm", "-D", "--defined-only", pm.LIB_PATH], capture_output=True, text=True, check=True)
+    exported = set(re.findall(r" T (pm_\w+)", out.stdout))
+    missing = declared() - exported
+    assert not missing, missing
+    L = pm.lib()
+    for n in declared():
+        assert hasattr(L, n)
+    # the Python mirror binds every declared entry point
+    assert declared() <= set(pm.SIGNATURES)
+
+
+def test_struct_layouts_match_c():
+    """Compiles a probe against the header and compares sizeof/offsetof."""
+    src = r'''
+#include <stdio.h>
+#include <stddef.h>
+#include "pumatch.h"
+int main(void){
+ printf("%zu %zu %zu %zu %zu %zu %zu %zu\n", sizeof(pm_graph_opts), sizeof(pm_graph_info), sizeof(pm_plan_desc),
+        sizeof(pm_run_opts), sizeof(pm_stats), offsetof(pm_run_opts, root_begin), offsetof(pm_run_opts, root_counts),
+        offsetof(pm_stats, kernel_ms));
+ return 0; }'''
+    import ctypes as C
+    import tempfile
+    d = tempfile.mkdtemp()
+    open(os.path.join(d, "p.c"), "w").write(src)
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), "-o", os.path.join(d, "p"), os.path.join(d, "p.c")],
+                   check=True)
+    vals = [int(x) for x in subprocess.run([os.path.join(d, "p")], capture_output=True, text=True).stdout.split()]
+    assert vals == [C.sizeof(pm.GraphOpts), C.sizeof(pm.GraphInfo), C.sizeof(pm.PlanDesc), C.sizeof(pm.RunOpts),
+                    C.sizeof(pm.Stats), pm.RunOpts.root_begin.offset, pm.RunOpts.root_counts.offset,
+                    pm.Stats.kernel_ms.offset]
+
+
+def test_strerror():
+    assert pm.lib().pm_strerror(pm.PM_ERR_NO_DEVICE) == b"no CUDA device"
+    assert pm.lib().pm_strerror(pm.PM_OK) == b"ok"
+
+
+@pytest.mark.skipif(torch.cuda.is_available(), reason="checks the no-GPU behaviour")
+def test_no_cpu_fallback():
+    with pytest.raises(pm.PmError) as e:
+        pm.Context(0)
+    assert e.value.status == pm.PM_ERR_NO_DEVICE
+    hg = pm.gen_chung_lu(100, 300, seed=1)
+    with pytest.raises(pm.PmError) as e:
+        pm.GraphPreprocessor.from_host(hg)
+    assert e.value.status == pm.PM_ERR_NO_DEVICE
+    # the drop-in CLI fails loudly too
+    gold = os.path.join(ROOT, "tests", "golden", "graphs", "cl400")
+    pat = os.path.join(ROOT, "tests", "golden", "_c4.g")
+    from pumatch_b200 import patterns as P
+    open(pat, "w").write(P.to_g(*P.cycle(4)))
+    try:
+        r = subprocess.run([pm.CLI_PATH, gold, pat], capture_output=True, text=True)
+        assert r.returncode != 0 and "no CUDA device" in r.stderr
+    finally:
+        os.remove(pat)
+
+
+def test_cli_usage():
+    r = subprocess.run([pm.CLI_PATH], capture_output=True, text=True)
+    assert r.returncode == 2 and "usage" in r.stderr
