@@ -92,6 +92,13 @@ pm_status pm_graph_from_device(int64_t n, int64_t n_adj, int32_t max_degree,
                                const uint8_t* d_labels, int device, pm_graph** out);
 
 pm_status pm_graph_get_info(const pm_graph* g, pm_graph_info* info);
+
+/* Paged graphs: the pages (indices of page_bytes-sized ranges of the adjacency
+ * array) the frame pool holds at the start of every run that is not cold --
+ * by default the first n_frames pages.  Replaces the reference's initial
+ * package build over the vertices past the device partition
+ * (src/buffer.cu:986-1060 create_buffer_from_graph). */
+pm_status pm_graph_set_resident_pages(pm_graph* g, const int64_t* pages, int64_t n);
 void pm_graph_close(pm_graph* g);
 
 /* Reader/writer of the reference's on-disk layout (src/graph.h:228-254,
@@ -174,6 +181,9 @@ pm_status pm_debug_roots(pm_ctx* ctx, const pm_graph* g, const pm_plan* p, int32
 
 pm_status pm_ctx_create(int device, pm_ctx** out);
 void pm_ctx_destroy(pm_ctx* ctx);
+/* The cudaStream_t (as void*) every matching launch of this context uses, so
+ * callers can order their own work and time it with events on it. */
+void* pm_ctx_stream(pm_ctx* ctx);
 
 typedef struct {
   int32_t truncate;         /* 0: exact.  >0: emulate the reference's
@@ -193,11 +203,14 @@ typedef struct {
   int64_t root_begin;       /* restrict to roots [root_begin, root_end) of
                                the reference-ordered root list; -1 = all     */
   int64_t root_end;
-  int32_t reserved_[4];
+  int32_t cold_cache;       /* paged mode: empty the frame pool before the run */
+  int32_t reserved_[3];
   uint64_t* root_counts;    /* optional device ptr: per-root counts (plan 0) */
   float* root_cost;         /* optional device ptr: per-root set-op bytes    */
   const int32_t* root_order;/* optional device ptr: process roots in this
                                order (learned binning); NULL = natural      */
+  float* root_reads;        /* optional device ptr: per-root adjacency-list
+                               reads (page touches when paged; plan 0)      */
 } pm_run_opts;
 
 void pm_run_opts_default(pm_run_opts* o);
@@ -229,6 +242,49 @@ typedef struct {
  * automorphism count when unlabeled, as test.cu:198 does). */
 pm_status pm_match(pm_ctx* ctx, const pm_graph* g, const pm_plan* const* plans, int nplans,
                    const pm_run_opts* opts, uint64_t* counts_out, pm_stats* stats_out);
+
+/* Prepared query: the batched multi-pattern launch built once -- root lists,
+ * arenas, plan upload and the persistent kernel captured in a CUDA graph --
+ * and replayed by each pm_query_run.  Same results as pm_match.  The graph
+ * and context must outlive the query. */
+typedef struct pm_query pm_query;
+pm_status pm_query_prepare(pm_ctx* ctx, const pm_graph* g, const pm_plan* const* plans, int nplans,
+                           const pm_run_opts* opts, pm_query** out);
+pm_status pm_query_run(pm_query* q, uint64_t* counts_out, pm_stats* stats_out);
+void pm_query_free(pm_query* q);
+
+/* ------------------------------------------------------------------ */
+/* Learned scheduler (no counterpart in the reference)                   */
+/* ------------------------------------------------------------------ */
+
+#define PM_MLP_IN 16
+#define PM_MLP_HIDDEN 64
+#define PM_MLP_OUT 2
+#define PM_MLP_PARAMS (PM_MLP_IN * PM_MLP_HIDDEN + PM_MLP_HIDDEN + PM_MLP_HIDDEN * PM_MLP_HIDDEN + \
+                       PM_MLP_HIDDEN + PM_MLP_HIDDEN * PM_MLP_OUT + PM_MLP_OUT)
+
+/* PM_MLP_IN features per root edge of plan p, in root-list order, into the
+ * device buffer d_features (cap rows); *n_roots gets the root count (call
+ * with d_features NULL to size the buffer). */
+pm_status pm_root_features(pm_ctx* ctx, const pm_graph* g, const pm_plan* p, float* d_features,
+                           int64_t cap, int64_t* n_roots);
+
+/* 16 -> 64 -> 64 -> 2 MLP, ReLU, BF16 weights with FP32 accumulation and FP32
+ * master weights (Adam).  Parameters are laid out W1[16][64] b1 W2[64][64] b2
+ * W3[64][2] b3 (input-major).  All data pointers are device pointers except
+ * the host weight/gradient buffers. */
+typedef struct pm_mlp pm_mlp;
+pm_status pm_mlp_create(int device, uint64_t seed, pm_mlp** out);
+void pm_mlp_free(pm_mlp* m);
+pm_status pm_mlp_forward(pm_mlp* m, const float* d_x, int64_t n, float* d_y);
+/* Mean-squared-error gradient over n samples into host_grad[PM_MLP_PARAMS]. */
+pm_status pm_mlp_gradient(pm_mlp* m, const float* d_x, const float* d_t, int64_t n, float* host_grad,
+                          float* loss_out);
+/* One Adam step on the batch (gradient, update, BF16 re-quantisation). */
+pm_status pm_mlp_train_step(pm_mlp* m, const float* d_x, const float* d_t, int64_t n, float lr,
+                            float* loss_out);
+pm_status pm_mlp_get_weights(pm_mlp* m, float* host_out);
+pm_status pm_mlp_set_weights(pm_mlp* m, const float* host_in);
 
 const char* pm_strerror(pm_status s);
 const char* pm_last_error(void);

@@ -61,8 +61,10 @@ class RunOpts(C.Structure):
     _fields_ = [("truncate", C.c_int32), ("warps_per_block", C.c_int32), ("blocks_per_sm", C.c_int32),
                 ("chunk", C.c_int32), ("split_level1", C.c_int32), ("shard_rank", C.c_int32),
                 ("shard_count", C.c_int32), ("use_graph", C.c_int32), ("timeout_ms", C.c_int32),
-                ("root_begin", C.c_int64), ("root_end", C.c_int64), ("reserved_", C.c_int32 * 4),
-                ("root_counts", C.c_void_p), ("root_cost", C.c_void_p), ("root_order", C.c_void_p)]
+                ("root_begin", C.c_int64), ("root_end", C.c_int64), ("cold_cache", C.c_int32),
+                ("reserved_", C.c_int32 * 3),
+                ("root_counts", C.c_void_p), ("root_cost", C.c_void_p), ("root_order", C.c_void_p),
+                ("root_reads", C.c_void_p)]
 
 
 class Stats(C.Structure):
@@ -88,6 +90,7 @@ SIGNATURES = {
     "pm_graph_from_host": (C.c_int, [C.c_int64, C.c_int64, _P, _P, _P, C.POINTER(GraphOpts), _PP]),
     "pm_graph_from_device": (C.c_int, [C.c_int64, C.c_int64, C.c_int32, _P, _P, _P, C.c_int, _PP]),
     "pm_graph_get_info": (C.c_int, [_P, C.POINTER(GraphInfo)]),
+    "pm_graph_set_resident_pages": (C.c_int, [_P, _P, C.c_int64]),
     "pm_graph_close": (None, [_P]),
     "pm_graph_read": (C.c_int, [C.c_char_p, C.c_int, C.POINTER(C.c_int64), C.POINTER(C.c_int64),
                                 C.POINTER(C.c_int32), _PP, _PP, _PP]),
@@ -106,9 +109,21 @@ SIGNATURES = {
     "pm_debug_roots": (C.c_int, [_P, _P, _P, _P, C.c_int64, C.POINTER(C.c_int64)]),
     "pm_ctx_create": (C.c_int, [C.c_int, _PP]),
     "pm_ctx_destroy": (None, [_P]),
+    "pm_ctx_stream": (C.c_void_p, [_P]),
     "pm_run_opts_default": (None, [C.POINTER(RunOpts)]),
     "pm_match": (C.c_int, [_P, _P, _PP, C.c_int, C.POINTER(RunOpts), C.POINTER(C.c_uint64),
                            C.POINTER(Stats)]),
+    "pm_query_prepare": (C.c_int, [_P, _P, _PP, C.c_int, C.POINTER(RunOpts), _PP]),
+    "pm_query_run": (C.c_int, [_P, C.POINTER(C.c_uint64), C.POINTER(Stats)]),
+    "pm_query_free": (None, [_P]),
+    "pm_root_features": (C.c_int, [_P, _P, _P, _P, C.c_int64, C.POINTER(C.c_int64)]),
+    "pm_mlp_create": (C.c_int, [C.c_int, C.c_uint64, _PP]),
+    "pm_mlp_free": (None, [_P]),
+    "pm_mlp_forward": (C.c_int, [_P, _P, C.c_int64, _P]),
+    "pm_mlp_gradient": (C.c_int, [_P, _P, _P, C.c_int64, _P, C.POINTER(C.c_float)]),
+    "pm_mlp_train_step": (C.c_int, [_P, _P, _P, C.c_int64, C.c_float, C.POINTER(C.c_float)]),
+    "pm_mlp_get_weights": (C.c_int, [_P, _P]),
+    "pm_mlp_set_weights": (C.c_int, [_P, _P]),
     "pm_strerror": (C.c_char_p, [C.c_int]),
     "pm_last_error": (C.c_char_p, []),
 }
@@ -314,6 +329,11 @@ class GraphPreprocessor:
         _check(lib().pm_graph_get_info(self._h, C.byref(gi)))
         return {k: getattr(gi, k) for k, _ in gi._fields_}
 
+    def set_resident_pages(self, pages) -> None:
+        """Paged graphs: pages the frame pool starts each warm run with."""
+        arr = np.ascontiguousarray(pages, dtype=np.int64)
+        _check(lib().pm_graph_set_resident_pages(self._h, arr.ctypes.data_as(C.c_void_p), len(arr)))
+
     def close(self) -> None:
         if self._h:
             lib().pm_graph_close(self._h)
@@ -346,6 +366,11 @@ class Context:
         except Exception:
             pass
 
+    @property
+    def stream_ptr(self) -> int:
+        """cudaStream_t of this context's launches (for torch.cuda.ExternalStream)."""
+        return lib().pm_ctx_stream(self._h) or 0
+
     def count_roots(self, g: GraphPreprocessor, p: PatternPreprocessor) -> int:
         n = C.c_int64()
         _check(lib().pm_count_roots(self._h, g._h, p._h, C.byref(n)))
@@ -359,26 +384,74 @@ class Context:
         _check(lib().pm_debug_roots(self._h, g._h, p._h, _ptr(out), n, C.byref(got)))
         return out[:n]
 
+    @staticmethod
+    def _opts(**kw) -> RunOpts:
+        o = RunOpts()
+        lib().pm_run_opts_default(C.byref(o))
+        for k, v in kw.items():
+            if k.endswith("_ptr"):
+                setattr(o, k[:-4], v or None)
+            else:
+                setattr(o, k, int(v))
+        return o
+
+    def prepare(self, g: GraphPreprocessor, patterns: Sequence[PatternPreprocessor], **kw) -> "Query":
+        """A prepared batched launch replayed from a CUDA graph (pm_query_*)."""
+        return Query(self, g, patterns, self._opts(**kw))
+
     def match(self, g: GraphPreprocessor, patterns: Sequence[PatternPreprocessor], *, truncate: int = 0,
               warps_per_block: int = 0, blocks_per_sm: int = 0, chunk: int = 0, split_level1: int = 0,
               shard_rank: int = 0, shard_count: int = 0, root_begin: int = -1, root_end: int = -1,
-              root_counts_ptr: int = 0, root_cost_ptr: int = 0, root_order_ptr: int = 0,
-              use_graph: bool = False):
+              root_counts_ptr: int = 0, root_cost_ptr: int = 0, root_order_ptr: int = 0, root_reads_ptr: int = 0,
+              use_graph: bool = False, timeout_ms: int = 0, cold_cache: bool = False):
         """Runs all patterns in one launch; returns (counts list, stats dict)."""
         o = RunOpts()
         lib().pm_run_opts_default(C.byref(o))
         o.truncate, o.warps_per_block, o.blocks_per_sm, o.chunk = truncate, warps_per_block, blocks_per_sm, chunk
         o.split_level1, o.shard_rank, o.shard_count = split_level1, shard_rank, shard_count
         o.root_begin, o.root_end, o.use_graph = root_begin, root_end, int(use_graph)
+        o.timeout_ms = timeout_ms
+        o.cold_cache = int(cold_cache)
         o.root_counts = root_counts_ptr or None
         o.root_cost = root_cost_ptr or None
         o.root_order = root_order_ptr or None
+        o.root_reads = root_reads_ptr or None
         k = len(patterns)
         arr = (C.c_void_p * k)(*[p._h.value for p in patterns])
         counts = (C.c_uint64 * k)()
         st = Stats()
         _check(lib().pm_match(self._h, g._h, C.cast(arr, _PP), k, C.byref(o), counts, C.byref(st)))
         return [int(x) for x in counts], st.as_dict()
+
+
+class Query:
+    """pm_query_prepare / pm_query_run / pm_query_free."""
+
+    def __init__(self, ctx: Context, g: GraphPreprocessor, patterns: Sequence[PatternPreprocessor], o: RunOpts):
+        self._keep = (ctx, g, list(patterns))
+        k = len(patterns)
+        arr = (C.c_void_p * k)(*[p._h.value for p in patterns])
+        h = C.c_void_p()
+        _check(lib().pm_query_prepare(ctx._h, g._h, C.cast(arr, _PP), k, C.byref(o), C.byref(h)))
+        self._h = h
+        self.k = k
+
+    def run(self):
+        counts = (C.c_uint64 * self.k)()
+        st = Stats()
+        _check(lib().pm_query_run(self._h, counts, C.byref(st)))
+        return [int(x) for x in counts], st.as_dict()
+
+    def close(self) -> None:
+        if self._h:
+            lib().pm_query_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def match(g: GraphPreprocessor, patterns, ctx: Optional[Context] = None, **kw):
@@ -394,6 +467,6 @@ def match(g: GraphPreprocessor, patterns, ctx: Optional[Context] = None, **kw):
 
 
 __all__ = [
-    "PmError", "HostGraph", "GraphPreprocessor", "PatternPreprocessor", "Context", "match",
+    "PmError", "HostGraph", "GraphPreprocessor", "PatternPreprocessor", "Context", "Query", "match",
     "gen_chung_lu", "gen_rmat", "gen_labels", "lib", "LIB_PATH", "CLI_PATH", "SIGNATURES",
 ]

@@ -29,6 +29,7 @@
 
 #include "pm_common.h"
 #include "pm_device.cuh"
+#include "pm_paging.cuh"
 
 namespace pm {
 const Plan* plan_of(const pm_plan* h);
@@ -56,45 +57,20 @@ static constexpr unsigned FULL = 0xffffffffu;
 __constant__ DPlan c_plans[PM_MAX_BATCH];
 
 __device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
 __device__ __forceinline__ unsigned lanemask_lt() {
   unsigned m;
   asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
   return m;
 }
 
-// First index of sorted A[0,len) whose element is >= ub: a 32-ary search,
-// one strided probe per lane per round (log32(len) rounds).
-__device__ __forceinline__ int warp_lower_bound(const int32_t* A, int len, int ub) {
-  const int lane = lane_id();
-  int lo = 0, hi = len;
-  while (hi - lo > 32) {
-    const int step = (hi - lo + 31) >> 5;
-    const long long idx = lo + (long long)lane * step;
-    const bool lt = idx < hi && A[idx] < ub;
-    const int k = __popc(__ballot_sync(FULL, lt));
-    if (k == 0) return lo;
-    const int nhi = min(hi, lo + k * step);
-    lo = lo + (k - 1) * step + 1;
-    hi = nhi;
-  }
-  const int idx = lo + lane;
-  const bool lt = idx < hi && A[idx] < ub;
-  return lo + __popc(__ballot_sync(FULL, lt));
-}
-
-// Membership of a in sorted B[0, len) by binary search (per lane).
-__device__ __forceinline__ bool bsearch_in(const int32_t* B, int len, int a) {
-  int lo = 0, hi = len;
-  while (lo < hi) {
-    const int mid = (lo + hi) >> 1;
-    if (B[mid] < a) lo = mid + 1; else hi = mid;
-  }
-  return lo < len && B[lo] == a;
-}
-
 struct MatchArgs {
   const uint64_t* rowptr;
-  const int32_t* colidx;
+  const int32_t* colidx;        // HBM residency
   const uint8_t* labels;
   int32_t n;
   int32_t nplans;
@@ -102,16 +78,18 @@ struct MatchArgs {
   int32_t chunk;
   int32_t shard_rank;
   int32_t shard_count;
-  int32_t split_min;          // donate level-1 ranges at least this long
-  int32_t pad0;
+  int32_t split_min;            // donate level-1 ranges at least this long
+  int32_t maxdeg;
   unsigned long long* cursors;  // [nplans]
   unsigned long long* counts;   // [nplans]
-  unsigned long long* stats;    // [8]
+  unsigned long long* stats;    // [16]
   unsigned int* status;
   int32_t* arena;
-  int64_t arena_words;          // per warp
+  int64_t arena_words;          // per warp, including the gather space
+  int64_t slot_words;           // per warp, slots only (gather space follows)
   unsigned long long* root_counts;
   float* root_cost;
+  float* root_reads;
   const int32_t* root_order;
   // donation ring: items (plan, root, begin, end) -- level-1 ranges
   int4* don_items;
@@ -121,10 +99,14 @@ struct MatchArgs {
   unsigned int* active;           // warps holding work (phase 1 or a donation)
   unsigned int total_warps;
   unsigned long long* don_tail;   // next slot to take
+  unsigned long long* heartbeat;  // bumped by busy warps
+  unsigned long long timeout_ns;  // hard limit on the launch; idle warps also give
+                                  // up after this long without a heartbeat
   DPaging pg;
 };
 
-enum { ST_SETOPS = 0, ST_BYTES = 1, ST_ROOTS = 2, ST_SPLITS = 3 };
+enum { ST_SETOPS = 0, ST_BYTES = 1, ST_ROOTS = 2, ST_SPLITS = 3, ST_HITS = 4, ST_MISSES = 5,
+       ST_ZC_BYTES = 6, ST_REQUESTS = 7, ST_EVICTIONS = 8, ST_DROPPED = 9 };
 
 struct WarpState {
   int32_t path[8];
@@ -133,13 +115,65 @@ struct WarpState {
   int32_t top[9];    // arena offset where level L's slots start
   int32_t off[16];
   int32_t size[16];
+  unsigned long long next_beat;  // setops value at which to bump the heartbeat
+  unsigned long long t_start;    // %globaltimer at kernel entry (ns)
+  int32_t pins[PM_MAX_LIST_PAGES];  // paged mode: frames pinned for a gather
 };
 
-// Adjacency list of v.  HBM residency: a slice of colidx.
-__device__ __forceinline__ const int32_t* adj(const MatchArgs& a, int v, int& len) {
+// Per-warp work counters (registers; flushed once at kernel exit).
+struct Work {
+  unsigned long long setops, bytes, reads;
+  unsigned int err;
+  PageCounters pc;
+};
+
+template <bool CG>
+__device__ __forceinline__ int32_t ld(const int32_t* p) {
+  if (CG) return __ldcg(p);  // frames are refilled during the launch: skip L1
+  return *p;
+}
+
+// First index of sorted A[0,len) whose element is >= ub: a 32-ary search,
+// one strided probe per lane per round (log32(len) rounds).
+template <bool CG>
+__device__ __forceinline__ int warp_lower_bound(const int32_t* A, int len, int ub) {
+  const int lane = lane_id();
+  int lo = 0, hi = len;
+  while (hi - lo > 32) {
+    const int step = (hi - lo + 31) >> 5;
+    const long long idx = lo + (long long)lane * step;
+    const bool lt = idx < hi && ld<CG>(A + idx) < ub;
+    const int k = __popc(__ballot_sync(FULL, lt));
+    if (k == 0) return lo;
+    const int nhi = min(hi, lo + k * step);
+    lo = lo + (k - 1) * step + 1;
+    hi = nhi;
+  }
+  const int idx = lo + lane;
+  const bool lt = idx < hi && ld<CG>(A + idx) < ub;
+  return lo + __popc(__ballot_sync(FULL, lt));
+}
+
+// Membership of x in sorted B[0, len) by binary search (per lane).
+template <bool CG>
+__device__ __forceinline__ bool bsearch_in(const int32_t* B, int len, int x) {
+  int lo = 0, hi = len;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (ld<CG>(B + mid) < x) lo = mid + 1; else hi = mid;
+  }
+  return lo < len && ld<CG>(B + lo) == x;
+}
+
+// Adjacency list of v: a slice of colidx in HBM, or resolved through the
+// page cache (frame, gathered copy, or host read).
+template <bool PAGED>
+__device__ __forceinline__ ListRef adj(const MatchArgs& a, WarpState& S, int v, int32_t* gather, Work& w) {
   const uint64_t b = a.rowptr[v];
-  len = (int)(a.rowptr[v + 1] - b);
-  return a.colidx + b;
+  const int len = (int)(a.rowptr[v + 1] - b);
+  w.reads++;
+  if (!PAGED) return ListRef{a.colidx + b, len, -1};
+  return paged_list(a.pg, b, len, gather, S.pins, w.pc);
 }
 
 // ---------------------------------------------------------------------
@@ -148,32 +182,30 @@ __device__ __forceinline__ const int32_t* adj(const MatchArgs& a, int v, int& le
 // (src/gpu_match.cu:409-812): returns the slot size (at the last level the
 // count), writes the slot to arena[top...] unless `last`.
 // ---------------------------------------------------------------------
-template <bool LABELED>
-__device__ int run_slot(const MatchArgs& a, const DPlan& P, WarpState& S, int32_t* arena, int L,
-                        int s, int top, bool last, unsigned long long& setops,
-                        unsigned long long& bytes, unsigned int& err) {
+template <bool LABELED, bool PAGED>
+__device__ int run_slot(const MatchArgs& a, const DPlan& P, WarpState& S, int32_t* arena, int L, int s,
+                        int top, bool last, Work& w) {
   const int lane = lane_id();
   const int kind = P.kind[s];
   const int vL = S.path[L];
-  const int32_t* A;
-  const int32_t* B = nullptr;
-  int lenA, lenB = 0;
+  int32_t* gatherA = arena + a.slot_words;
+  int32_t* gatherB = gatherA + a.maxdeg;
+  ListRef RA, RB{nullptr, 0, -1};
   if (kind != SLOT_COPY) {
-    A = adj(a, vL, lenA);
+    RA = adj<PAGED>(a, S, vL, gatherA, w);
   } else if (L > 1) {
-    A = arena + S.off[P.parent[s]];
-    lenA = S.size[P.parent[s]];
+    RA = ListRef{arena + S.off[P.parent[s]], S.size[P.parent[s]], -1};
   } else {
-    A = adj(a, S.path[0], lenA);
+    RA = adj<PAGED>(a, S, S.path[0], gatherA, w);
   }
   if (kind == SLOT_INTERSECT) {
-    if (L > 1) {
-      B = arena + S.off[P.parent[s]];
-      lenB = S.size[P.parent[s]];
-    } else {
-      B = adj(a, S.path[0], lenB);
-    }
+    if (L > 1) RB = ListRef{arena + S.off[P.parent[s]], S.size[P.parent[s]], -1};
+    else RB = adj<PAGED>(a, S, S.path[0], gatherB, w);
   }
+  const int32_t* A = RA.p;
+  const int32_t* B = RB.p;
+  int lenA = RA.len;
+  const int lenB = RB.len;
 
   // symmetry-breaking upper bound (unlabeled only, src/gpu_match.cu:426-458)
   if (!LABELED && P.partial[s]) {
@@ -186,26 +218,26 @@ __device__ int run_slot(const MatchArgs& a, const DPlan& P, WarpState& S, int32_
       else if (ub < v) ub = v;
     }
     if (ub == -1) ub = INT_MAX;
-    if (ub != INT_MAX) lenA = warp_lower_bound(A, lenA, (int)ub);
+    if (ub != INT_MAX) lenA = warp_lower_bound<PAGED>(A, lenA, (int)ub);
   }
 
   const int T = a.T;
   int scan = lenA;
   const bool fresh_unl = (!LABELED && kind == SLOT_FRESH);
   if (fresh_unl && T && scan > T) scan = T;  // first pass keeps A's prefix
-  if (!last && top + scan > a.arena_words) {
-    err |= DEV_ARENA_OVERFLOW;
-    return 0;
+  int cnt = 0;
+  if (!last && top + scan > a.slot_words) {
+    w.err |= DEV_ARENA_OVERFLOW;
+    scan = 0;
   }
   int32_t* out = arena + top;
   const uint32_t mask = P.slot_labels[s];
-  int cnt = 0;
   for (int base = 0; base < scan; base += 32) {
     const int i = base + lane;
     const bool valid = i < scan;
-    const int x = valid ? A[i] : 0;
+    const int x = valid ? ld<PAGED>(A + i) : 0;
     bool keep = valid;
-    if (kind == SLOT_INTERSECT && keep) keep = bsearch_in(B, lenB, x);
+    if (kind == SLOT_INTERSECT && keep) keep = bsearch_in<PAGED>(B, lenB, x);
     if (LABELED) {
       if (keep) keep = (mask >> a.labels[x]) & 1u;
     } else if (kind == SLOT_COPY) {
@@ -221,20 +253,24 @@ __device__ int run_slot(const MatchArgs& a, const DPlan& P, WarpState& S, int32_
     cnt += __popc(bal);
     if (T && cnt >= T && !fresh_unl) break;  // result is the first T survivors
   }
+  if (PAGED) {
+    __syncwarp();
+    unpin(a.pg, RA);
+    unpin(a.pg, RB);
+  }
   if (T && cnt > T) cnt = T;
-  setops++;
-  bytes += 4ull * (unsigned long long)(lenA + lenB + cnt) + (LABELED ? (unsigned long long)lenA : 0ull);
+  w.setops++;
+  w.bytes += 4ull * (unsigned long long)(lenA + lenB + cnt) + (LABELED ? (unsigned long long)lenA : 0ull);
   return cnt;
 }
 
 // Computes every slot of level L; returns the arena top after them.
-template <bool LABELED>
-__device__ __forceinline__ int run_level(const MatchArgs& a, const DPlan& P, WarpState& S,
-                                         int32_t* arena, int L, unsigned long long& setops,
-                                         unsigned long long& bytes, unsigned int& err) {
+template <bool LABELED, bool PAGED>
+__device__ __forceinline__ int run_level(const MatchArgs& a, const DPlan& P, WarpState& S, int32_t* arena,
+                                         int L, Work& w) {
   int top = S.top[L];
   for (int s = P.level_begin[L]; s < P.level_begin[L + 1]; s++) {
-    const int sz = run_slot<LABELED>(a, P, S, arena, L, s, top, false, setops, bytes, err);
+    const int sz = run_slot<LABELED, PAGED>(a, P, S, arena, L, s, top, false, w);
     if (lane_id() == 0) { S.off[s] = top; S.size[s] = sz; }
     top += sz;
   }
@@ -246,19 +282,17 @@ __device__ __forceinline__ int run_level(const MatchArgs& a, const DPlan& P, War
 // Depth-first enumeration below a root edge, over level-1 candidates
 // [b1, e1) (e1 < 0: all).  Restates match() (src/gpu_match.cu:855-1047)
 // without deferral: every branch is finished where it starts.
-template <bool LABELED>
-__device__ unsigned long long dfs_root(const MatchArgs& a, const DPlan& P, WarpState& S,
-                                       int32_t* arena, int v0, int v1, int b1, int e1,
-                                       bool may_split, int plan_id, int root_id,
-                                       unsigned long long& setops, unsigned long long& bytes,
-                                       unsigned int& err) {
+template <bool LABELED, bool PAGED>
+__device__ unsigned long long dfs_root(const MatchArgs& a, const DPlan& P, WarpState& S, int32_t* arena,
+                                       int v0, int v1, int b1, int e1, bool may_split, int plan_id,
+                                       int root_id, Work& w) {
   const int lane = lane_id();
   const int n = P.nnodes;
   if (lane == 0) { S.path[0] = v0; S.path[1] = v1; S.top[1] = 0; }
   __syncwarp();
-  if (n == 3) return (unsigned long long)run_slot<LABELED>(a, P, S, arena, 1, P.level_begin[1], 0, true, setops, bytes, err);
-  run_level<LABELED>(a, P, S, arena, 1, setops, bytes, err);
-  if (err) return 0;
+  if (n == 3) return (unsigned long long)run_slot<LABELED, PAGED>(a, P, S, arena, 1, P.level_begin[1], 0, true, w);
+  run_level<LABELED, PAGED>(a, P, S, arena, 1, w);
+  if (w.err) return 0;
   unsigned long long cnt = 0;
   const int m1 = P.level_begin[1];
   int end1 = S.size[m1];
@@ -268,11 +302,11 @@ __device__ unsigned long long dfs_root(const MatchArgs& a, const DPlan& P, WarpS
   int L = 1;
   while (true) {
     const int m = P.level_begin[L];
-    int it = S.iter[L];
+    const int it = S.iter[L];
     int iend = (L == 1) ? S.iend[1] : S.size[m];
     // donate the upper half of a long level-1 range when warps are idle
-    if (L == 1 && may_split && a.split_min > 0 && iend - it >= a.split_min) {
-      int give = 0;
+    if (L == 1 && may_split && a.split_min > 0 && iend - it >= max(a.split_min, 2)) {
+      int gave = 0, newend = iend;
       if (lane == 0) {
         const unsigned int act = *((volatile unsigned int*)a.active);
         const unsigned long long head = *((volatile unsigned long long*)a.don_head);
@@ -280,19 +314,33 @@ __device__ unsigned long long dfs_root(const MatchArgs& a, const DPlan& P, WarpS
         // only while some warps idle and fewer ranges are queued than idle warps
         if (act < a.total_warps && head - tail < (unsigned long long)(a.total_warps - act)) {
           const unsigned long long slot = atomicAdd(a.don_head, 1ull);
-          const int mid = it + (iend - it) / 2;
+          const int mid = it + (iend - it) / 2;  // it < mid < iend
           a.don_items[slot & a.don_mask] = make_int4(plan_id, root_id, mid, iend);
           __threadfence();
           atomicExch(&a.don_ready[slot & a.don_mask], slot + 1);
           atomicAdd(&a.stats[ST_SPLITS], 1ull);
-          give = mid;
+          gave = 1;
+          newend = mid;
+          S.iend[1] = mid;
         }
       }
-      give = __shfl_sync(FULL, give, 0);
-      if (give) {
-        iend = give;
-        if (lane == 0) S.iend[1] = give;
-        __syncwarp();
+      gave = __shfl_sync(FULL, gave, 0);
+      newend = __shfl_sync(FULL, newend, 0);
+      if (gave) iend = newend;
+      __syncwarp();
+    }
+    // liveness signal for idle warps and the kernel-wide deadline, checked
+    // once per ~1024 set operations
+    if (w.setops >= S.next_beat) {
+      int late = 0;
+      if (lane == 0) {
+        atomicAdd(a.heartbeat, 1ull);
+        S.next_beat = w.setops + 1024;
+        late = (global_ns() - S.t_start) > a.timeout_ns;
+      }
+      if (__shfl_sync(FULL, late, 0)) {
+        w.err |= DEV_TIMEOUT;
+        return 0;
       }
     }
     if (it < iend) {
@@ -300,14 +348,14 @@ __device__ unsigned long long dfs_root(const MatchArgs& a, const DPlan& P, WarpS
       if (lane == 0) { S.iter[L] = it + 1; S.path[L + 1] = v; }
       __syncwarp();
       if (L + 1 == n - 2) {
-        cnt += (unsigned long long)run_slot<LABELED>(a, P, S, arena, L + 1, P.last_slot, S.top[L + 1], true, setops, bytes, err);
+        cnt += (unsigned long long)run_slot<LABELED, PAGED>(a, P, S, arena, L + 1, P.last_slot, S.top[L + 1], true, w);
       } else {
         L++;
-        run_level<LABELED>(a, P, S, arena, L, setops, bytes, err);
+        run_level<LABELED, PAGED>(a, P, S, arena, L, w);
         if (lane == 0) S.iter[L] = 0;
         __syncwarp();
       }
-      if (err) return 0;
+      if (w.err) return 0;
     } else {
       L--;
       if (L < 1) break;
@@ -355,21 +403,24 @@ __device__ bool take_donation(const MatchArgs& a, int4& item) {
   return got != 0;
 }
 
-template <bool LABELED>
-__global__ void __launch_bounds__(256) match_kernel(MatchArgs a) {
+template <bool LABELED, bool PAGED>
+__global__ void __launch_bounds__(512) match_kernel(MatchArgs a) {
   extern __shared__ WarpState smem_state[];
   const int lane = lane_id();
   const int wib = threadIdx.x >> 5;
   WarpState& S = smem_state[wib];
+  if (lane == 0) { S.next_beat = 0; S.t_start = global_ns(); }
+  __syncwarp();
   const long long gw = (long long)blockIdx.x * (blockDim.x >> 5) + wib;
   int32_t* arena = a.arena + gw * a.arena_words;
-  unsigned long long setops = 0, bytes = 0, roots = 0;
-  unsigned int err = 0;
+  Work w;
+  memset(&w, 0, sizeof(w));
+  unsigned long long roots = 0;
   const int np = a.nplans;
   int p = (int)(gw % np);
   int exhausted = 0;
   // phase 1: root chunks from the per-plan cursors
-  while (exhausted < np && !err) {
+  while (exhausted < np && !w.err) {
     const DPlan& P = c_plans[p];
     const unsigned long long nchunks = (unsigned long long)((P.nroots + a.chunk - 1) / a.chunk);
     unsigned long long c = 0;
@@ -385,18 +436,18 @@ __global__ void __launch_bounds__(256) match_kernel(MatchArgs a) {
     const long long rb = (long long)gc * a.chunk;
     const long long re = min((long long)P.nroots, rb + a.chunk);
     unsigned long long local = 0;
-    for (long long r = rb; r < re && !err; r++) {
+    for (long long r = rb; r < re && !w.err; r++) {
       const long long rid = a.root_order ? (long long)a.root_order[r] : r;
       const int2 e = P.roots[rid];
-      const unsigned long long b0 = bytes;
-      const unsigned long long c0 = LABELED
-          ? dfs_root<true>(a, P, S, arena, e.x, e.y, 0, -1, true, p, (int)rid, setops, bytes, err)
-          : dfs_root<false>(a, P, S, arena, e.x, e.y, 0, -1, true, p, (int)rid, setops, bytes, err);
+      const unsigned long long b0 = w.bytes, r0 = w.reads;
+      const unsigned long long c0 =
+          dfs_root<LABELED, PAGED>(a, P, S, arena, e.x, e.y, 0, -1, true, p, (int)rid, w);
       local += c0;
       roots++;
       if (lane == 0 && p == 0) {
         if (a.root_counts) atomicAdd(&a.root_counts[rid], c0);
-        if (a.root_cost) atomicAdd(&a.root_cost[rid], (float)(bytes - b0 + 8));
+        if (a.root_cost) atomicAdd(&a.root_cost[rid], (float)(w.bytes - b0 + 8));
+        if (a.root_reads) atomicAdd(&a.root_reads[rid], (float)(w.reads - r0));
       }
     }
     if (lane == 0 && local) atomicAdd(&a.counts[p], local);
@@ -406,51 +457,66 @@ __global__ void __launch_bounds__(256) match_kernel(MatchArgs a) {
   __threadfence();
   if (lane == 0) atomicSub(a.active, 1u);
   __syncwarp();
-  for (long long idle_spins = 0; !err;) {
+  unsigned long long last_beat = 0, last_change = global_ns();
+  while (!w.err) {
     int4 item;
     if (take_donation(a, item)) {
       const DPlan& P = c_plans[item.x];
       const int2 e = P.roots[item.y];
-      const unsigned long long b0 = bytes;
-      const unsigned long long c0 = LABELED
-          ? dfs_root<true>(a, P, S, arena, e.x, e.y, item.z, item.w, true, item.x, item.y, setops, bytes, err)
-          : dfs_root<false>(a, P, S, arena, e.x, e.y, item.z, item.w, true, item.x, item.y, setops, bytes, err);
+      const unsigned long long b0 = w.bytes, r0 = w.reads;
+      const unsigned long long c0 =
+          dfs_root<LABELED, PAGED>(a, P, S, arena, e.x, e.y, item.z, item.w, true, item.x, item.y, w);
       if (lane == 0) {
         if (c0) atomicAdd(&a.counts[item.x], c0);
         if (item.x == 0) {
           if (a.root_counts) atomicAdd(&a.root_counts[item.y], c0);
-          if (a.root_cost) atomicAdd(&a.root_cost[item.y], (float)(bytes - b0));
+          if (a.root_cost) atomicAdd(&a.root_cost[item.y], (float)(w.bytes - b0));
+          if (a.root_reads) atomicAdd(&a.root_reads[item.y], (float)(w.reads - r0));
         }
         __threadfence();
         atomicSub(a.active, 1u);
       }
       __syncwarp();
-      idle_spins = 0;
+      last_change = global_ns();
       continue;
     }
     unsigned int act = 0;
-    unsigned long long head = 0, tail = 0;
+    unsigned long long head = 0, tail = 0, beat = 0;
     if (lane == 0) {
       act = *((volatile unsigned int*)a.active);
       __threadfence();
       head = *((volatile unsigned long long*)a.don_head);
       tail = *((volatile unsigned long long*)a.don_tail);
+      beat = *((volatile unsigned long long*)a.heartbeat);
     }
     act = __shfl_sync(FULL, act, 0);
     head = __shfl_sync(FULL, head, 0);
     tail = __shfl_sync(FULL, tail, 0);
+    beat = __shfl_sync(FULL, beat, 0);
     if (act == 0 && tail >= head) break;
-    if (++idle_spins > (1ll << 28)) {  // bounded polling; the host sees DEV_TIMEOUT
+    // bounded wait: give up (and report DEV_TIMEOUT) when no warp has made
+    // progress for timeout_ns
+    const unsigned long long now = global_ns();
+    if (beat != last_beat) { last_beat = beat; last_change = now; }
+    else if (now - last_change > a.timeout_ns) {
       if (lane == 0) atomicOr(a.status, (unsigned)DEV_TIMEOUT);
       break;
     }
-    __nanosleep(256);
+    __nanosleep(1000);
   }
   if (lane == 0) {
-    atomicAdd(&a.stats[ST_SETOPS], setops);
-    atomicAdd(&a.stats[ST_BYTES], bytes + 8ull * roots);
+    atomicAdd(&a.stats[ST_SETOPS], w.setops);
+    atomicAdd(&a.stats[ST_BYTES], w.bytes + 8ull * roots);
     atomicAdd(&a.stats[ST_ROOTS], roots);
-    if (err) atomicOr(a.status, err);
+    if (PAGED) {
+      atomicAdd(&a.stats[ST_HITS], w.pc.hits);
+      atomicAdd(&a.stats[ST_MISSES], w.pc.misses);
+      atomicAdd(&a.stats[ST_ZC_BYTES], w.pc.zc_bytes);
+      atomicAdd(&a.stats[ST_REQUESTS], w.pc.requests);
+      atomicAdd(&a.stats[ST_EVICTIONS], w.pc.evictions);
+      atomicAdd(&a.stats[ST_DROPPED], w.pc.dropped);
+    }
+    if (w.err) atomicOr(a.status, w.err);
   }
 }
 
@@ -585,6 +651,19 @@ int64_t arena_words_for(const Plan& p, int32_t maxdeg, int T) {
 
 }  // namespace
 
+namespace pm {
+// Fills g->d_maxnbrdeg from an adjacency array the device can read (HBM or
+// mapped host memory).
+pm_status compute_maxnbrdeg(pm_graph* g, const int32_t* colidx) {
+  if (g->n > 0) {
+    maxnbrdeg_kernel<<<2048, 256>>>(g->d_rowptr, colidx, g->n, g->d_maxnbrdeg);
+    CK(cudaGetLastError());
+    CK(cudaDeviceSynchronize());
+  }
+  return PM_OK;
+}
+}  // namespace pm
+
 static pm_status graph_finish(pm_graph* g) {
   // per-vertex max neighbour degree, used by the root filter
   CK(cudaMalloc(&g->d_maxnbrdeg, sizeof(int32_t) * std::max<int64_t>(g->n, 1)));
@@ -601,8 +680,8 @@ namespace pm {
 pm_status paged_place(pm_graph* g, const int32_t* colidx, const pm_graph_opts* o);
 pm_status paged_maxnbrdeg(pm_graph* g);
 void paged_release(pm_graph* g);
-pm_status paged_prepare(pm_ctx* ctx, pm_graph* g, DPaging* out);
-pm_status paged_service_start(pm_ctx* ctx, pm_graph* g, const DPaging& pg);
+pm_status paged_prepare(pm_ctx* ctx, pm_graph* g, bool cold, DPaging* out);
+pm_status paged_service_start(pm_ctx* ctx, pm_graph* g);
 pm_status paged_service_stop(pm_ctx* ctx, pm_graph* g, pm_stats* st);
 }  // namespace pm
 
@@ -753,6 +832,8 @@ extern "C" pm_status pm_ctx_create(int device, pm_ctx** out) {
   return PM_OK;
 }
 
+extern "C" void* pm_ctx_stream(pm_ctx* c) { return c ? (void*)c->stream : nullptr; }
+
 extern "C" void pm_ctx_destroy(pm_ctx* c) {
   if (!c) return;
   cudaSetDevice(c->device);
@@ -779,7 +860,9 @@ extern "C" void pm_run_opts_default(pm_run_opts* o) {
 
 // Builds the root list of plan p into ctx->d_roots + offset; returns count.
 static pm_status build_roots(pm_ctx* c, const pm_graph* g, const Plan& p, size_t offset_roots,
-                             int64_t* count, bool count_only) {
+                             int64_t* count, bool count_only, int2** roots_buf = nullptr,
+                             size_t* roots_bytes = nullptr) {
+  if (!roots_buf) { roots_buf = &c->d_roots; roots_bytes = &c->roots_bytes; }
   const int64_t n = g->n;
   if (n == 0) { *count = 0; return PM_OK; }
   if (c->vbuf_n < (size_t)n + 1) {
@@ -808,20 +891,20 @@ static pm_status build_roots(pm_ctx* c, const pm_graph* g, const Plan& p, size_t
   CK(cudaStreamSynchronize(c->stream));
   *count = total;
   if (count_only) return PM_OK;
-  const size_t want = sizeof(int2) * (offset_roots + (size_t)total);
-  if (c->roots_bytes < want) {
+  const size_t want = sizeof(int2) * (offset_roots + (size_t)total) + sizeof(int2);
+  if (*roots_bytes < want) {
     // grow, keeping the roots of earlier plans
     int2* nr = nullptr;
     CK(cudaMalloc(&nr, want + want / 4));
-    if (c->d_roots && offset_roots)
-      CK(cudaMemcpyAsync(nr, c->d_roots, sizeof(int2) * offset_roots, cudaMemcpyDeviceToDevice, c->stream));
+    if (*roots_buf && offset_roots)
+      CK(cudaMemcpyAsync(nr, *roots_buf, sizeof(int2) * offset_roots, cudaMemcpyDeviceToDevice, c->stream));
     CK(cudaStreamSynchronize(c->stream));
-    free_dev(c->d_roots);
-    c->d_roots = nr;
-    c->roots_bytes = want + want / 4;
+    free_dev(*roots_buf);
+    *roots_buf = nr;
+    *roots_bytes = want + want / 4;
   }
   roots_kernel<true><<<4 * c->nsm, 256, 0, c->stream>>>(g->d_rowptr, colidx, g->d_labels, g->d_maxnbrdeg, n, f,
-                                                         nullptr, c->d_voff, c->d_roots + offset_roots);
+                                                         nullptr, c->d_voff, *roots_buf + offset_roots);
   CK(cudaGetLastError());
   return PM_OK;
 }
@@ -835,6 +918,19 @@ extern "C" pm_status pm_count_roots(pm_ctx* c, const pm_graph* g, const pm_plan*
 }
 
 namespace pm {
+// Root list of one plan in the context's root buffer (valid until the next
+// call that builds roots on this context).
+pm_status root_list_for(pm_ctx* c, const pm_graph* g, const pm_plan* ph, const int2** roots, int64_t* n) {
+  const Plan* p = plan_of(ph);
+  if (p->labeled && !g->labeled) return fail(PM_ERR_INVALID, "labeled plan on an unlabeled graph");
+  CK(cudaSetDevice(c->device));
+  pm_status st = build_roots(c, g, *p, 0, n, false);
+  if (st != PM_OK) return st;
+  CK(cudaStreamSynchronize(c->stream));
+  *roots = c->d_roots;
+  return PM_OK;
+}
+
 // Exposed for tests through pm_debug_roots: copies the root list of one plan.
 pm_status debug_roots(pm_ctx* c, const pm_graph* g, const Plan& p, int32_t* out_pairs, int64_t cap, int64_t* count) {
   pm_status st = build_roots(c, g, p, 0, count, false);
@@ -853,86 +949,106 @@ extern "C" pm_status pm_debug_roots(pm_ctx* c, const pm_graph* g, const pm_plan*
   return debug_roots(c, g, *plan_of(ph), out_pairs, cap, count);
 }
 
-extern "C" pm_status pm_match(pm_ctx* c, const pm_graph* g, const pm_plan* const* plans, int nplans,
-                              const pm_run_opts* opts, uint64_t* counts_out, pm_stats* stats_out) {
-  if (!c || !g || !plans || nplans < 1 || !counts_out) return fail(PM_ERR_INVALID, "pm_match: bad arguments");
-  if (nplans > PM_MAX_BATCH) return fail(PM_ERR_INVALID, "pm_match: at most %d plans per launch", PM_MAX_BATCH);
-  pm_run_opts o;
-  pm_run_opts_default(&o);
-  if (opts) o = *opts;
+// One prepared persistent launch: plans, roots, geometry, kernel arguments.
+struct Launch {
+  bool labeled = false, paged = false, cold = false;
+  int nplans = 0;
+  const Plan* plans[PM_MAX_BATCH];
+  DPlan dp[PM_MAX_BATCH];
+  MatchArgs a;
+  int blocks = 0, threads = 0;
+  size_t smem = 0;
+  void (*kfn)(MatchArgs) = nullptr;
+  int64_t warps = 0;
+  size_t ctl_words = 0;
+  unsigned int active0 = 0;  // initial active-warp count (host staging)
+};
+
+static constexpr unsigned kDonSlots = 1u << 16;
+static constexpr int kCtlRead = 32 + 32 + 16 + 1;  // cursors, counts, stats, status word
+
+// Validates the plans and options, builds the root lists into *roots,
+// sizes the persistent grid and the arenas, and fills L.  Buffers are grown
+// as needed (they belong to the caller: the context for pm_match, the query
+// for pm_query_prepare).
+static pm_status setup_launch(pm_ctx* c, const pm_graph* g, const pm_plan* const* plans, int nplans,
+                              const pm_run_opts& o, int2** roots, size_t* roots_bytes, int32_t** arena,
+                              size_t* arena_bytes, unsigned long long** ctl, size_t* ctl_bytes, Launch* L) {
+  if (nplans < 1 || nplans > PM_MAX_BATCH) return fail(PM_ERR_INVALID, "between 1 and %d plans per launch", PM_MAX_BATCH);
   CK(cudaSetDevice(c->device));
-  const bool labeled = plan_of(plans[0])->labeled != 0;
+  L->labeled = plan_of(plans[0]) && plan_of(plans[0])->labeled != 0;
   for (int i = 0; i < nplans; i++) {
     const Plan* p = plan_of(plans[i]);
-    if (!p) return fail(PM_ERR_INVALID, "pm_match: null plan %d", i);
-    if ((p->labeled != 0) != labeled) return fail(PM_ERR_INVALID, "pm_match: plans mix labeled and unlabeled modes");
+    if (!p) return fail(PM_ERR_INVALID, "null plan %d", i);
+    if ((p->labeled != 0) != L->labeled) return fail(PM_ERR_INVALID, "plans mix labeled and unlabeled modes");
     if (p->labeled && !g->labeled) return fail(PM_ERR_INVALID, "labeled plan on an unlabeled graph");
+    L->plans[i] = p;
   }
+  L->nplans = nplans;
   if (o.root_order && nplans != 1) return fail(PM_ERR_INVALID, "root_order needs a single plan");
   const int T = std::max(0, o.truncate);
   const int wpb = o.warps_per_block > 0 ? o.warps_per_block : 8;
-  if (wpb > 8 || (wpb & (wpb - 1))) return fail(PM_ERR_INVALID, "warps_per_block must be 1,2,4 or 8");
+  if (wpb > 16 || (wpb & (wpb - 1))) return fail(PM_ERR_INVALID, "warps_per_block must be 1,2,4,8 or 16");
   const int chunk = o.chunk > 0 ? o.chunk : 16;
   const int shard_count = o.shard_count > 1 ? o.shard_count : 1;
   if (o.shard_rank < 0 || o.shard_rank >= shard_count) return fail(PM_ERR_INVALID, "bad shard_rank");
-
-  cudaEvent_t e0 = c->ev[0], e1 = c->ev[1], e2 = c->ev[2];
-  CK(cudaEventRecord(e0, c->stream));
+  L->paged = g->residency == PM_RESIDENT_PAGED;
+  L->cold = o.cold_cache != 0;
 
   // root lists, concatenated
-  DPlan dp[PM_MAX_BATCH];
   size_t off = 0;
   int64_t arena_words = 64;
   for (int i = 0; i < nplans; i++) {
-    const Plan& p = *plan_of(plans[i]);
+    const Plan& p = *L->plans[i];
     int64_t cnt = 0;
-    pm_status st = build_roots(c, g, p, off, &cnt, false);
+    pm_status st = build_roots(c, g, p, off, &cnt, false, roots, roots_bytes);
     if (st != PM_OK) return st;
-    dp[i] = to_dplan(p);
-    dp[i].nroots = cnt;
+    L->dp[i] = to_dplan(p);
+    L->dp[i].nroots = cnt;
     arena_words = std::max(arena_words, arena_words_for(p, g->maxdeg, T));
     off += (size_t)cnt;
   }
   off = 0;
   for (int i = 0; i < nplans; i++) {
-    int64_t b = 0, e = dp[i].nroots;
+    int64_t b = 0, e = L->dp[i].nroots;
     if (o.root_begin >= 0) b = std::min<int64_t>(o.root_begin, e);
     if (o.root_end >= 0) e = std::min<int64_t>(o.root_end, e);
     if (e < b) e = b;
-    dp[i].roots = c->d_roots + off + b;
-    off += (size_t)dp[i].nroots;
-    dp[i].nroots = e - b;
+    L->dp[i].roots = *roots + off + b;
+    off += (size_t)L->dp[i].nroots;
+    L->dp[i].nroots = e - b;
   }
-  CK(cudaMemcpyToSymbolAsync(c_plans, dp, sizeof(DPlan) * nplans, 0, cudaMemcpyHostToDevice, c->stream));
-  CK(cudaEventRecord(e1, c->stream));
+  const int64_t slot_words = arena_words;
+  if (L->paged) arena_words += 2 * (int64_t)g->maxdeg + 64;  // gather space for multi-page lists
 
   // launch geometry: persistent, occupancy-limited
-  const int threads = wpb * 32;
-  const size_t smem = sizeof(WarpState) * wpb;
+  L->threads = wpb * 32;
+  L->smem = sizeof(WarpState) * wpb;
+  L->kfn = L->labeled ? (L->paged ? match_kernel<true, true> : match_kernel<true, false>)
+                      : (L->paged ? match_kernel<false, true> : match_kernel<false, false>);
   int per_sm = 0;
-  if (labeled) CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, match_kernel<true>, threads, smem));
-  else CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, match_kernel<false>, threads, smem));
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, L->kfn, L->threads, L->smem));
   if (o.blocks_per_sm > 0) per_sm = std::min(per_sm, o.blocks_per_sm);
   per_sm = std::max(per_sm, 1);
-  int blocks = c->nsm * per_sm;
-  int64_t warps = (int64_t)blocks * wpb;
-  // cap the arena to half of free memory by reducing resident warps
+  L->blocks = c->nsm * per_sm;
+  L->warps = (int64_t)L->blocks * wpb;
+  // keep the arenas within half of the free memory by trimming resident warps
   size_t free_b = 0, total_b = 0;
   CK(cudaMemGetInfo(&free_b, &total_b));
-  while (blocks > c->nsm && (size_t)(warps * arena_words * 4) > free_b / 2) {
-    blocks -= c->nsm;
-    warps = (int64_t)blocks * wpb;
+  free_b += *arena_bytes;
+  while (L->blocks > c->nsm && (size_t)(L->warps * arena_words * 4) > free_b / 2) {
+    L->blocks -= c->nsm;
+    L->warps = (int64_t)L->blocks * wpb;
   }
-  pm_status st = ensure((void**)&c->d_arena, &c->arena_bytes, (size_t)(warps * arena_words * 4));
+  pm_status st = ensure((void**)arena, arena_bytes, (size_t)(L->warps * arena_words * 4));
+  if (st != PM_OK) return st;
+  // control block: cursors[32] counts[32] stats[16] status/active head tail
+  // heartbeat, donation ready[] and items[]
+  L->ctl_words = 32 + 32 + 16 + 8 + kDonSlots + 2 * kDonSlots;
+  st = ensure((void**)ctl, ctl_bytes, L->ctl_words * 8);
   if (st != PM_OK) return st;
 
-  // control block: cursors[32] counts[32] stats[8] status idle head tail ring...
-  const unsigned don_slots = 1u << 16;
-  const size_t ctl_words = 32 + 32 + 8 + 4 + 2 * don_slots + don_slots * 2;
-  st = ensure((void**)&c->d_ctl, &c->ctl_bytes, ctl_words * 8);
-  if (st != PM_OK) return st;
-  CK(cudaMemsetAsync(c->d_ctl, 0, ctl_words * 8, c->stream));
-  MatchArgs a;
+  MatchArgs& a = L->a;
   memset(&a, 0, sizeof(a));
   a.rowptr = g->d_rowptr;
   a.colidx = g->d_colidx;
@@ -944,59 +1060,219 @@ extern "C" pm_status pm_match(pm_ctx* c, const pm_graph* g, const pm_plan* const
   a.shard_rank = o.shard_rank;
   a.shard_count = shard_count;
   a.split_min = o.split_level1 == 0 ? 64 : (o.split_level1 < 0 ? 0 : o.split_level1);
-  unsigned long long* w = c->d_ctl;
+  a.maxdeg = g->maxdeg;
+  unsigned long long* w = *ctl;
   a.cursors = w; w += 32;
   a.counts = w; w += 32;
-  a.stats = w; w += 8;
+  a.stats = w; w += 16;
   a.status = (unsigned int*)w;
   a.active = (unsigned int*)w + 1; w += 1;
   a.don_head = w; w += 1;
-  a.don_tail = w; w += 2;
-  a.don_ready = w; w += don_slots;
-  a.don_items = (int4*)w; w += 2 * don_slots;
-  a.don_mask = don_slots - 1;
-  a.total_warps = (unsigned int)warps;
-  a.arena = c->d_arena;
+  a.don_tail = w; w += 1;
+  a.heartbeat = w; w += 5;
+  a.don_ready = w; w += kDonSlots;
+  a.don_items = (int4*)w; w += 2 * kDonSlots;
+  a.don_mask = kDonSlots - 1;
+  a.total_warps = (unsigned int)L->warps;
+  a.arena = *arena;
   a.arena_words = arena_words;
+  a.slot_words = slot_words;
   a.root_counts = (unsigned long long*)o.root_counts;
   a.root_cost = o.root_cost;
+  a.root_reads = o.root_reads;
   a.root_order = o.root_order;
-  if (g->residency == PM_RESIDENT_PAGED) return fail(PM_ERR_INVALID, "paged residency is not available in this build");
+  a.timeout_ns = (unsigned long long)(o.timeout_ms > 0 ? o.timeout_ms : 600000) * 1000000ull;
+  L->active0 = (unsigned int)L->warps;
+  if (L->paged) {
+    st = paged_prepare(c, const_cast<pm_graph*>(g), L->cold, &a.pg);
+    if (st != PM_OK) return st;
+  }
+  return PM_OK;
+}
 
-  // every warp starts active (it holds root chunks until the cursors run dry)
-  c->h_active = (unsigned int)warps;
-  CK(cudaMemcpyAsync(a.active, &c->h_active, sizeof(unsigned int), cudaMemcpyHostToDevice, c->stream));
-  CK(cudaEventRecord(e1, c->stream));
-  if (labeled) match_kernel<true><<<blocks, threads, smem, c->stream>>>(a);
-  else match_kernel<false><<<blocks, threads, smem, c->stream>>>(a);
+// Enqueues one launch on the context stream: plan upload, control reset,
+// the persistent kernel between events eb/ee, and the read-back of counts,
+// stats and status into host_ctl.  Capturable into a CUDA graph (host_ctl,
+// dp_src and active_src must then be pinned).
+static pm_status enqueue_launch(pm_ctx* c, Launch& L, const DPlan* dp_src, const unsigned int* active_src,
+                                unsigned long long* host_ctl, cudaEvent_t eb, cudaEvent_t ee) {
+  CK(cudaMemcpyToSymbolAsync(c_plans, dp_src, sizeof(DPlan) * L.nplans, 0, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemsetAsync(L.a.cursors, 0, L.ctl_words * 8, c->stream));
+  CK(cudaMemcpyAsync(L.a.active, active_src, sizeof(unsigned int), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaEventRecord(eb, c->stream));
+  L.kfn<<<L.blocks, L.threads, L.smem, c->stream>>>(L.a);
   CK(cudaGetLastError());
-  CK(cudaEventRecord(e2, c->stream));
-  unsigned long long host_ctl[32 + 32 + 8 + 1];
-  CK(cudaMemcpyAsync(host_ctl, c->d_ctl, sizeof(host_ctl), cudaMemcpyDeviceToHost, c->stream));
-  CK(cudaStreamSynchronize(c->stream));
-  const unsigned int status = (unsigned int)(host_ctl[72] & 0xffffffffu);
-  for (int i = 0; i < nplans; i++) {
-    const Plan& p = *plan_of(plans[i]);
+  CK(cudaEventRecord(ee, c->stream));
+  CK(cudaMemcpyAsync(host_ctl, L.a.cursors, sizeof(unsigned long long) * kCtlRead, cudaMemcpyDeviceToHost,
+                     c->stream));
+  return PM_OK;
+}
+
+// Turns the read-back control words into counts, stats and a status.
+static pm_status finish_launch(const Launch& L, const unsigned long long* host_ctl, float kernel_ms, float roots_ms,
+                               const pm_stats& pst, uint64_t* counts_out, pm_stats* stats_out) {
+  const unsigned int status = (unsigned int)(host_ctl[80] & 0xffffffffu);
+  for (int i = 0; i < L.nplans; i++) {
+    const Plan& p = *L.plans[i];
     counts_out[i] = host_ctl[32 + i] * (p.labeled ? 1ull : (uint64_t)p.multiplicity);
   }
   if (stats_out) {
-    memset(stats_out, 0, sizeof(*stats_out));
-    stats_out->set_ops = host_ctl[64 + ST_SETOPS];
-    stats_out->alg_bytes = host_ctl[64 + ST_BYTES];
-    stats_out->n_roots = host_ctl[64 + ST_ROOTS];
-    stats_out->splits = host_ctl[64 + ST_SPLITS];
-    float ms = 0;
-    CK(cudaEventElapsedTime(&ms, e1, e2));
-    stats_out->kernel_ms = ms;
-    CK(cudaEventElapsedTime(&ms, e0, e1));
-    stats_out->roots_ms = ms;
-    stats_out->grid_blocks = blocks;
-    stats_out->block_threads = threads;
-    stats_out->arena_bytes = (uint64_t)(warps * arena_words * 4);
-    stats_out->device_status = status;
+    pm_stats& so = *stats_out;
+    so = pst;
+    const unsigned long long* stt = host_ctl + 64;
+    so.set_ops = stt[ST_SETOPS];
+    so.alg_bytes = stt[ST_BYTES];
+    so.n_roots = stt[ST_ROOTS];
+    so.splits = stt[ST_SPLITS];
+    so.page_hits = stt[ST_HITS];
+    so.page_misses = stt[ST_MISSES];
+    so.zero_copy_bytes = stt[ST_ZC_BYTES];
+    so.evictions = stt[ST_EVICTIONS];
+    so.kernel_ms = kernel_ms;
+    so.roots_ms = roots_ms;
+    so.grid_blocks = L.blocks;
+    so.block_threads = L.threads;
+    so.arena_bytes = (uint64_t)(L.warps * L.a.arena_words * 4);
+    so.device_status = status;
   }
   if (status & DEV_ARENA_OVERFLOW) return fail(PM_ERR_INTERNAL, "device: candidate set exceeded the warp arena");
-  if (status & DEV_TIMEOUT) return fail(PM_ERR_TIMEOUT, "device: a bounded wait gave up");
+  if (status & DEV_TIMEOUT) return fail(PM_ERR_TIMEOUT, "device: the launch hit its time limit or a bounded wait gave up");
   if (status) return fail(PM_ERR_INTERNAL, "device status 0x%x", status);
   return PM_OK;
+}
+
+// Runs an enqueued launch to completion, with the page service around it.
+template <class Enqueue>
+static pm_status run_launch(pm_ctx* c, const pm_graph* g, Launch& L, Enqueue enqueue, pm_stats* pst) {
+  memset(pst, 0, sizeof(*pst));
+  if (L.paged) {
+    pm_status st = paged_service_start(c, const_cast<pm_graph*>(g));
+    if (st != PM_OK) return st;
+  }
+  pm_status est = enqueue();
+  cudaError_t sync_err = cudaStreamSynchronize(c->stream);
+  if (L.paged) {
+    pm_status sst = paged_service_stop(c, const_cast<pm_graph*>(g), pst);
+    if (sst != PM_OK && est == PM_OK && sync_err == cudaSuccess) return sst;
+  }
+  if (est != PM_OK) return est;
+  CK(sync_err);
+  return PM_OK;
+}
+
+extern "C" pm_status pm_match(pm_ctx* c, const pm_graph* g, const pm_plan* const* plans, int nplans,
+                              const pm_run_opts* opts, uint64_t* counts_out, pm_stats* stats_out) {
+  if (!c || !g || !plans || nplans < 1 || !counts_out) return fail(PM_ERR_INVALID, "pm_match: bad arguments");
+  pm_run_opts o;
+  pm_run_opts_default(&o);
+  if (opts) o = *opts;
+  CK(cudaSetDevice(c->device));
+  cudaEvent_t e0 = c->ev[0], e1 = c->ev[1], e2 = c->ev[2];
+  CK(cudaEventRecord(e0, c->stream));
+  std::unique_ptr<Launch> L(new Launch);
+  pm_status st = setup_launch(c, g, plans, nplans, o, &c->d_roots, &c->roots_bytes, &c->d_arena, &c->arena_bytes,
+                              &c->d_ctl, &c->ctl_bytes, L.get());
+  if (st != PM_OK) return st;
+  c->h_active = L->active0;
+  unsigned long long host_ctl[kCtlRead];
+  pm_stats pst;
+  st = run_launch(c, g, *L, [&]() { return enqueue_launch(c, *L, L->dp, &c->h_active, host_ctl, e1, e2); }, &pst);
+  if (st != PM_OK) return st;
+  float kms = 0, rms = 0;
+  CK(cudaEventElapsedTime(&kms, e1, e2));
+  CK(cudaEventElapsedTime(&rms, e0, e1));
+  return finish_launch(*L, host_ctl, kms, rms, pst, counts_out, stats_out);
+}
+
+// ---------------------------------------------------------------------
+// Prepared queries: the root lists, arenas and launch sequence are built
+// once; each run replays the launch captured in a CUDA graph.
+// ---------------------------------------------------------------------
+struct pm_query {
+  pm_ctx* c = nullptr;
+  const pm_graph* g = nullptr;
+  Launch L;
+  int2* d_roots = nullptr;
+  size_t roots_bytes = 0;
+  int32_t* d_arena = nullptr;
+  size_t arena_bytes = 0;
+  unsigned long long* d_ctl = nullptr;
+  size_t ctl_bytes = 0;
+  DPlan* h_dp = nullptr;              // pinned
+  unsigned int* h_active = nullptr;   // pinned
+  unsigned long long* h_ctl = nullptr;  // pinned
+  cudaEvent_t eb = nullptr, ee = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  float roots_ms = 0;
+};
+
+extern "C" void pm_query_free(pm_query* q) {
+  if (!q) return;
+  cudaSetDevice(q->c->device);
+  if (q->exec) cudaGraphExecDestroy(q->exec);
+  if (q->graph) cudaGraphDestroy(q->graph);
+  if (q->eb) cudaEventDestroy(q->eb);
+  if (q->ee) cudaEventDestroy(q->ee);
+  free_dev(q->d_roots);
+  free_dev(q->d_arena);
+  free_dev(q->d_ctl);
+  if (q->h_dp) cudaFreeHost(q->h_dp);
+  if (q->h_active) cudaFreeHost(q->h_active);
+  if (q->h_ctl) cudaFreeHost(q->h_ctl);
+  delete q;
+}
+
+extern "C" pm_status pm_query_prepare(pm_ctx* c, const pm_graph* g, const pm_plan* const* plans, int nplans,
+                                      const pm_run_opts* opts, pm_query** out) {
+  if (!c || !g || !plans || !out) return fail(PM_ERR_INVALID, "pm_query_prepare: bad arguments");
+  pm_run_opts o;
+  pm_run_opts_default(&o);
+  if (opts) o = *opts;
+  CK(cudaSetDevice(c->device));
+  std::unique_ptr<pm_query, void (*)(pm_query*)> q(new pm_query, pm_query_free);
+  q->c = c;
+  q->g = g;
+  CK(cudaEventRecord(c->ev[0], c->stream));
+  pm_status st = setup_launch(c, g, plans, nplans, o, &q->d_roots, &q->roots_bytes, &q->d_arena, &q->arena_bytes,
+                              &q->d_ctl, &q->ctl_bytes, &q->L);
+  if (st != PM_OK) return st;
+  CK(cudaEventRecord(c->ev[1], c->stream));
+  CK(cudaEventSynchronize(c->ev[1]));
+  CK(cudaEventElapsedTime(&q->roots_ms, c->ev[0], c->ev[1]));
+  CK(cudaMallocHost(&q->h_dp, sizeof(DPlan) * PM_MAX_BATCH));
+  CK(cudaMallocHost(&q->h_active, sizeof(unsigned int)));
+  CK(cudaMallocHost(&q->h_ctl, sizeof(unsigned long long) * kCtlRead));
+  memcpy(q->h_dp, q->L.dp, sizeof(DPlan) * q->L.nplans);
+  *q->h_active = q->L.active0;
+  CK(cudaEventCreate(&q->eb));
+  CK(cudaEventCreate(&q->ee));
+  CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+  pm_status est = enqueue_launch(c, q->L, q->h_dp, q->h_active, q->h_ctl, q->eb, q->ee);
+  cudaError_t cerr = cudaStreamEndCapture(c->stream, &q->graph);
+  if (est != PM_OK) return est;
+  CK(cerr);
+  CK(cudaGraphInstantiate(&q->exec, q->graph, 0));
+  *out = q.release();
+  return PM_OK;
+}
+
+extern "C" pm_status pm_query_run(pm_query* q, uint64_t* counts_out, pm_stats* stats_out) {
+  if (!q || !counts_out) return fail(PM_ERR_INVALID, "pm_query_run: bad arguments");
+  pm_ctx* c = q->c;
+  CK(cudaSetDevice(c->device));
+  if (q->L.paged) {
+    DPaging pg;
+    pm_status st = paged_prepare(c, const_cast<pm_graph*>(q->g), q->L.cold, &pg);  // reset the page table
+    if (st != PM_OK) return st;
+  }
+  pm_stats pst;
+  pm_status st = run_launch(c, q->g, q->L, [&]() -> pm_status {
+    CK(cudaGraphLaunch(q->exec, c->stream));
+    return PM_OK;
+  }, &pst);
+  if (st != PM_OK) return st;
+  float kms = 0;
+  CK(cudaEventElapsedTime(&kms, q->eb, q->ee));
+  return finish_launch(q->L, q->h_ctl, kms, q->roots_ms, pst, counts_out, stats_out);
 }

@@ -35,28 +35,31 @@ struct DPlan {
 };
 
 // Page cache of the adjacency array (paged residency).  A page is a fixed
-// range of colidx; frames are page-sized slots of a device pool.
+// power-of-two range of colidx; frames are page-sized slots of a device pool.
 struct DPaging {
-  int32_t enabled;
-  int32_t page_shift;             // log2(ints per page)
+  int32_t page_shift;              // log2(ints per page)
+  int32_t pad0;
   int64_t n_pages;
   int64_t n_frames;
-  int32_t* page_frame;            // [n_pages]: frame, or PAGE_ABSENT / PAGE_LOADING
-  int32_t* frame_page;            // [n_frames]: page held, -1 free
-  int32_t* frame_pin;             // [n_frames]: readers in flight
-  uint8_t* frame_ref;             // [n_frames]: CLOCK reference bits
-  int32_t* frames;                // [n_frames << page_shift]
-  const int32_t* host_colidx;     // device-visible pointer to pinned host colidx
-  unsigned long long* clock_hand;
-  // fault ring in mapped pinned host memory: (page, frame) requests
-  int2* ring;                     // device-visible pointer
+  int32_t* page_frame;             // [n_pages]: frame, or PAGE_ABSENT/LOADING/EVICTING
+  int32_t* frame_page;             // [n_frames]: page held, -1 never used
+  int32_t* frame_pin;              // [n_frames]: readers in flight
+  uint8_t* frame_ref;              // [n_frames]: CLOCK reference bits
+  int32_t* frames;                 // [n_frames << page_shift]
+  const int32_t* host_colidx;      // device-visible pointer to pinned host colidx
+  unsigned long long* clock_hand;  // device
+  unsigned long long* next_free;   // device: frames handed out so far
+  unsigned long long* ring_head;   // device: ring slots reserved
+  int2* ring;                      // mapped host: (page, frame) requests
+  unsigned long long* ring_seq;    // mapped host: slot + 1 once written
+  unsigned long long* host_tail;   // mapped host: slots the host consumed
   unsigned int ring_mask;
-  unsigned int* ring_head;        // device counter (slots claimed)
-  volatile unsigned int* ring_published; // host-visible: per slot sequence
-  unsigned long long* counters;   // [hits, misses, zero_copy_bytes, loads, evictions]
+  unsigned int pad1;
 };
 
 enum : int32_t { PAGE_ABSENT = -1, PAGE_LOADING = -2 };
+
+struct PagedState;  // host-side page service state (pm_paging.cu)
 
 }  // namespace pm
 
@@ -74,16 +77,12 @@ struct pm_graph {
   uint8_t* d_labels = nullptr;
   int32_t* d_maxnbrdeg = nullptr;
   uint64_t device_bytes = 0;
-  // paged residency
-  int32_t* h_colidx = nullptr;   // pinned, mapped
-  int32_t* h_colidx_dev = nullptr;
+  // paged residency (pm_paging.cu)
+  int32_t* h_colidx = nullptr;     // pinned, mapped copy of the adjacency array
+  int32_t* h_colidx_dev = nullptr; // its device-visible address
   uint32_t page_ints = 0;
   int64_t n_pages = 0, n_frames = 0;
-  int32_t* d_frames = nullptr;
-  int32_t* d_page_frame = nullptr;
-  int32_t* d_frame_page = nullptr;
-  int32_t* d_frame_pin = nullptr;
-  uint8_t* d_frame_ref = nullptr;
+  pm::PagedState* ps = nullptr;
 };
 
 struct pm_ctx {

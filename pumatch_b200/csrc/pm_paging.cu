@@ -1,10 +1,303 @@
-// pm_paging.cu -- placeholder for the paged (out-of-HBM) residency.
+// pm_paging.cu -- host side of the paged residency: placement of the
+// adjacency array in pinned host memory, the device page table and frame pool,
+// and the service thread that turns page requests into H2D copies.
+//
+// Replaces the reference's host packaging threads (src/buffer.cu:1218-1389
+// cpu_process_all_vertices, :1580-1645 cpu_process_multiple_queue, :873-929
+// copy_packages_to_gpu; test.cu:160-169).  Differences by design:
+//   * one service thread per graph, not one per CUDA block, and it never
+//     handshakes with the kernel -- the kernel keeps running on host reads
+//     while a page is in flight;
+//   * copies come from pinned memory (true async DMA) on a side stream, one
+//     cudaMemcpyAsync per page plus one 4-byte copy that publishes the page
+//     table entry after it (same stream, so it lands after the data);
+//   * eviction is decided on the device (CLOCK over reference bits, skipping
+//     pinned frames), so the host never overwrites a frame a warp is reading.
+#include <atomic>
+#include <chrono>
+#include <cstring>
+#include <thread>
+#include <vector>
+
 #include "pm_device.cuh"
+#include "pm_paging.cuh"
+
+#define CKP(call)                                                                             \
+  do {                                                                                        \
+    cudaError_t e_ = (call);                                                                  \
+    if (e_ != cudaSuccess)                                                                    \
+      return fail(PM_ERR_CUDA, "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+  } while (0)
 
 namespace pm {
-pm_status paged_place(pm_graph*, const int32_t*, const pm_graph_opts*) {
-  return fail(PM_ERR_INVALID, "paged residency is not available in this build");
+
+pm_status compute_maxnbrdeg(pm_graph* g, const int32_t* colidx);
+
+struct PagedState {
+  int device = 0;
+  int32_t* frames = nullptr;
+  int32_t* page_frame = nullptr;
+  int32_t* frame_page = nullptr;
+  int32_t* frame_pin = nullptr;
+  uint8_t* frame_ref = nullptr;
+  unsigned long long* dctl = nullptr;  // [0] clock hand, [1] next free, [2] ring head
+  // mapped pinned host memory
+  int2* ring = nullptr;
+  unsigned long long* ring_seq = nullptr;
+  unsigned long long* host_tail = nullptr;
+  int2* ring_dev = nullptr;
+  unsigned long long* ring_seq_dev = nullptr;
+  unsigned long long* host_tail_dev = nullptr;
+  unsigned int ring_slots = 1u << 16;
+  int32_t* stage = nullptr;  // pinned: stage[f] = f, source of page-table publishes
+  int64_t prefilled = 0;     // frames 0..prefilled-1 hold the initial resident pages
+  int32_t* init_pf = nullptr;  // pinned [n_pages]: page -> frame at the start of a run
+  int32_t* init_fp = nullptr;  // pinned [n_frames]: frame -> page at the start of a run
+  // service thread
+  std::thread th;
+  std::atomic<bool> stop{false};
+  cudaStream_t copy_stream = nullptr;
+  unsigned long long tail = 0;
+  unsigned long long loaded = 0, h2d_bytes = 0, noops = 0;
+  cudaError_t err = cudaSuccess;
+};
+
+static void release_state(PagedState* s) {
+  if (!s) return;
+  cudaFree(s->frames);
+  cudaFree(s->page_frame);
+  cudaFree(s->frame_page);
+  cudaFree(s->frame_pin);
+  cudaFree(s->frame_ref);
+  cudaFree(s->dctl);
+  cudaFreeHost(s->ring);
+  cudaFreeHost(s->ring_seq);
+  cudaFreeHost(s->host_tail);
+  cudaFreeHost(s->stage);
+  cudaFreeHost(s->init_pf);
+  cudaFreeHost(s->init_fp);
+  if (s->copy_stream) cudaStreamDestroy(s->copy_stream);
+  delete s;
 }
-pm_status paged_maxnbrdeg(pm_graph*) { return PM_ERR_INVALID; }
-void paged_release(pm_graph*) {}
+
+// Resets the table to the initial residency (frames 0..prefilled-1 hold the
+// pages init_fp names), or to an empty pool when cold.  The initial pages are
+// (re)copied into their frames, since the last run may have evicted them.
+static pm_status reset_table(pm_graph* g, cudaStream_t st, bool cold) {
+  PagedState* s = g->ps;
+  const int64_t pre = cold ? 0 : s->prefilled;
+  if (pre > 0) {
+    CKP(cudaMemcpyAsync(s->page_frame, s->init_pf, sizeof(int32_t) * g->n_pages, cudaMemcpyHostToDevice, st));
+    CKP(cudaMemcpyAsync(s->frame_page, s->init_fp, sizeof(int32_t) * g->n_frames, cudaMemcpyHostToDevice, st));
+    const size_t pb = (size_t)g->page_ints * 4;
+    for (int64_t f = 0; f < pre;) {
+      // coalesce runs of consecutive pages in consecutive frames into one copy
+      int64_t e = f + 1;
+      while (e < pre && s->init_fp[e] == s->init_fp[e - 1] + 1) e++;
+      const int64_t first = (int64_t)s->init_fp[f] * g->page_ints;
+      const size_t bytes = std::min<size_t>((size_t)(e - f) * pb, sizeof(int32_t) * (size_t)(g->nadj - first));
+      CKP(cudaMemcpyAsync((char*)s->frames + (size_t)f * pb, g->h_colidx + first, bytes, cudaMemcpyHostToDevice, st));
+      f = e;
+    }
+  } else {
+    CKP(cudaMemsetAsync(s->page_frame, 0xff, sizeof(int32_t) * g->n_pages, st));  // PAGE_ABSENT
+    CKP(cudaMemsetAsync(s->frame_page, 0xff, sizeof(int32_t) * g->n_frames, st));
+  }
+  CKP(cudaMemsetAsync(s->frame_pin, 0, sizeof(int32_t) * g->n_frames, st));
+  CKP(cudaMemsetAsync(s->frame_ref, 0, g->n_frames, st));
+  unsigned long long h[4] = {0, (unsigned long long)pre, 0, 0};
+  CKP(cudaMemcpyAsync(s->dctl, h, sizeof(h), cudaMemcpyHostToDevice, st));
+  CKP(cudaStreamSynchronize(st));
+  s->tail = 0;
+  *(volatile unsigned long long*)s->host_tail = 0;
+  memset(s->ring_seq, 0, sizeof(unsigned long long) * s->ring_slots);
+  return PM_OK;
+}
+
+pm_status paged_place(pm_graph* g, const int32_t* colidx, const pm_graph_opts* o) {
+  uint32_t pb = o->page_bytes ? o->page_bytes : (64u << 10);
+  if (pb < 4096 || (pb & (pb - 1))) return fail(PM_ERR_INVALID, "page_bytes must be a power of two >= 4096");
+  std::unique_ptr<PagedState> s(new PagedState);
+  s->device = g->device;
+  const int64_t nadj = g->nadj;
+  g->page_ints = pb / 4;
+  int shift = 0;
+  while ((1u << shift) < g->page_ints) shift++;
+  g->n_pages = (nadj + g->page_ints - 1) / g->page_ints;
+  g->n_frames = std::min<int64_t>((int64_t)(o->frame_pool_bytes / pb), g->n_pages);
+  if (g->n_frames < 1 && g->n_pages > 0) g->n_frames = 1;
+  // adjacency in pinned, mapped host memory
+  CKP(cudaHostAlloc((void**)&g->h_colidx, sizeof(int32_t) * std::max<int64_t>(nadj, 1),
+                    cudaHostAllocMapped | cudaHostAllocPortable));
+  if (nadj) {
+    const int64_t kBlock = 1 << 24;
+#pragma omp parallel for schedule(static)
+    for (int64_t b = 0; b < (nadj + kBlock - 1) / kBlock; b++) {
+      const int64_t e = std::min(nadj, (b + 1) * kBlock);
+      memcpy(g->h_colidx + b * kBlock, colidx + b * kBlock, sizeof(int32_t) * (e - b * kBlock));
+    }
+  }
+  CKP(cudaHostGetDevicePointer((void**)&g->h_colidx_dev, g->h_colidx, 0));
+  // device page table and frame pool
+  const size_t fbytes = (size_t)g->n_frames * pb;
+  CKP(cudaMalloc(&s->frames, std::max<size_t>(fbytes, 4)));
+  CKP(cudaMalloc(&s->page_frame, sizeof(int32_t) * std::max<int64_t>(g->n_pages, 1)));
+  CKP(cudaMalloc(&s->frame_page, sizeof(int32_t) * std::max<int64_t>(g->n_frames, 1)));
+  CKP(cudaMalloc(&s->frame_pin, sizeof(int32_t) * std::max<int64_t>(g->n_frames, 1)));
+  CKP(cudaMalloc(&s->frame_ref, std::max<int64_t>(g->n_frames, 1)));
+  CKP(cudaMalloc(&s->dctl, sizeof(unsigned long long) * 4));
+  g->device_bytes += fbytes + 4 * g->n_pages + 9 * g->n_frames;
+  // request ring, consumer cursor and publish staging in mapped host memory
+  CKP(cudaHostAlloc((void**)&s->ring, sizeof(int2) * s->ring_slots, cudaHostAllocMapped | cudaHostAllocPortable));
+  CKP(cudaHostAlloc((void**)&s->ring_seq, sizeof(unsigned long long) * s->ring_slots,
+                    cudaHostAllocMapped | cudaHostAllocPortable));
+  CKP(cudaHostAlloc((void**)&s->host_tail, 64, cudaHostAllocMapped | cudaHostAllocPortable));
+  CKP(cudaHostAlloc((void**)&s->stage, sizeof(int32_t) * std::max<int64_t>(g->n_frames, 1), cudaHostAllocPortable));
+  for (int64_t f = 0; f < g->n_frames; f++) s->stage[f] = (int32_t)f;
+  CKP(cudaHostGetDevicePointer((void**)&s->ring_dev, s->ring, 0));
+  CKP(cudaHostGetDevicePointer((void**)&s->ring_seq_dev, s->ring_seq, 0));
+  CKP(cudaHostGetDevicePointer((void**)&s->host_tail_dev, s->host_tail, 0));
+  CKP(cudaStreamCreateWithFlags(&s->copy_stream, cudaStreamNonBlocking));
+  // warm start: the first pages of the array, the way the reference keeps the
+  // first 60% of the edges on the device (test.cu:22-43)
+  CKP(cudaHostAlloc((void**)&s->init_pf, sizeof(int32_t) * std::max<int64_t>(g->n_pages, 1), cudaHostAllocPortable));
+  CKP(cudaHostAlloc((void**)&s->init_fp, sizeof(int32_t) * std::max<int64_t>(g->n_frames, 1), cudaHostAllocPortable));
+  s->prefilled = g->n_frames;
+  for (int64_t p = 0; p < g->n_pages; p++) s->init_pf[p] = p < g->n_frames ? (int32_t)p : PAGE_ABSENT;
+  for (int64_t f = 0; f < g->n_frames; f++) s->init_fp[f] = (int32_t)f;
+  g->ps = s.release();
+  return reset_table(g, g->ps->copy_stream, false);
+}
+
+pm_status paged_maxnbrdeg(pm_graph* g) { return compute_maxnbrdeg(g, g->h_colidx_dev); }
+
+void paged_release(pm_graph* g) {
+  if (g->ps) {
+    if (g->ps->th.joinable()) {
+      g->ps->stop = true;
+      g->ps->th.join();
+    }
+    release_state(g->ps);
+    g->ps = nullptr;
+  }
+  if (g->h_colidx) cudaFreeHost(g->h_colidx);
+  g->h_colidx = nullptr;
+}
+
+pm_status paged_prepare(pm_ctx* c, pm_graph* g, bool cold, DPaging* out) {
+  PagedState* s = g->ps;
+  if (!s) return fail(PM_ERR_INTERNAL, "paged graph without page state");
+  pm_status st = reset_table(g, s->copy_stream, cold);
+  if (st != PM_OK) return st;
+  (void)c;
+  memset(out, 0, sizeof(*out));
+  int shift = 0;
+  while ((1u << shift) < g->page_ints) shift++;
+  out->page_shift = shift;
+  out->n_pages = g->n_pages;
+  out->n_frames = g->n_frames;
+  out->page_frame = s->page_frame;
+  out->frame_page = s->frame_page;
+  out->frame_pin = s->frame_pin;
+  out->frame_ref = s->frame_ref;
+  out->frames = s->frames;
+  out->host_colidx = g->h_colidx_dev;
+  out->clock_hand = s->dctl;
+  out->next_free = s->dctl + 1;
+  out->ring_head = s->dctl + 2;
+  out->ring = s->ring_dev;
+  out->ring_seq = s->ring_seq_dev;
+  out->host_tail = s->host_tail_dev;
+  out->ring_mask = s->ring_slots - 1;
+  return PM_OK;
+}
+
+// Drains posted requests: copy page -> frame, then publish the entry.
+static void service_loop(pm_graph* g) {
+  PagedState* s = g->ps;
+  cudaSetDevice(s->device);
+  const size_t pb = (size_t)g->page_ints * 4;
+  const int64_t nadj = g->nadj;
+  const unsigned mask = s->ring_slots - 1;
+  for (;;) {
+    int got = 0;
+    while (*(volatile unsigned long long*)&s->ring_seq[s->tail & mask] == s->tail + 1) {
+      std::atomic_thread_fence(std::memory_order_acquire);
+      const volatile int* slot = (const volatile int*)&s->ring[s->tail & mask];
+      const int2 req = make_int2(slot[0], slot[1]);
+      s->tail++;
+      got++;
+      if (req.x < 0) { s->noops++; continue; }
+      const int64_t first = (int64_t)req.x * g->page_ints;
+      const size_t bytes = std::min<size_t>(pb, sizeof(int32_t) * (size_t)(nadj - first));
+      cudaError_t e = cudaMemcpyAsync((char*)s->frames + (size_t)req.y * pb, g->h_colidx + first, bytes,
+                                      cudaMemcpyHostToDevice, s->copy_stream);
+      if (e == cudaSuccess)
+        e = cudaMemcpyAsync(s->page_frame + req.x, s->stage + req.y, sizeof(int32_t), cudaMemcpyHostToDevice,
+                            s->copy_stream);
+      if (e != cudaSuccess) {
+        // the page stays LOADING: readers keep using host reads, counts stay exact
+        s->err = e;
+        continue;
+      }
+      s->loaded++;
+      s->h2d_bytes += bytes;
+    }
+    if (got) {
+      std::atomic_thread_fence(std::memory_order_release);
+      *(volatile unsigned long long*)s->host_tail = s->tail;
+      continue;
+    }
+    if (s->stop.load(std::memory_order_acquire)) break;
+    std::this_thread::sleep_for(std::chrono::microseconds(20));
+  }
+  cudaStreamSynchronize(s->copy_stream);
+}
+
+pm_status paged_service_start(pm_ctx* c, pm_graph* g) {
+  (void)c;
+  PagedState* s = g->ps;
+  s->stop = false;
+  s->loaded = s->h2d_bytes = s->noops = 0;
+  s->err = cudaSuccess;
+  s->th = std::thread(service_loop, g);
+  return PM_OK;
+}
+
+// Called after the kernel finished: every request it posted is already in the
+// ring, so draining once more and joining completes all of them.
+pm_status paged_service_stop(pm_ctx* c, pm_graph* g, pm_stats* st) {
+  (void)c;
+  PagedState* s = g->ps;
+  s->stop = true;
+  if (s->th.joinable()) s->th.join();
+  st->pages_loaded = s->loaded;
+  st->h2d_page_bytes = s->h2d_bytes;
+  if (s->err != cudaSuccess)
+    return fail(PM_ERR_CUDA, "page service copy failed: %s", cudaGetErrorString(s->err));
+  return PM_OK;
+}
+
 }  // namespace pm
+
+// Chooses the pages the frame pool starts each (non-cold) run with -- e.g.
+// the pages a cost model predicts the hottest.  Pages beyond the pool size
+// are ignored; duplicates are an error.
+extern "C" pm_status pm_graph_set_resident_pages(pm_graph* g, const int64_t* pages, int64_t n) {
+  using namespace pm;
+  if (!g || (n > 0 && !pages) || n < 0) return fail(PM_ERR_INVALID, "pm_graph_set_resident_pages: bad arguments");
+  if (g->residency != PM_RESIDENT_PAGED || !g->ps) return fail(PM_ERR_INVALID, "graph is not paged");
+  PagedState* s = g->ps;
+  CKP(cudaSetDevice(g->device));
+  const int64_t k = std::min<int64_t>(n, g->n_frames);
+  std::vector<int32_t> pf((size_t)g->n_pages, PAGE_ABSENT);
+  for (int64_t f = 0; f < k; f++) {
+    if (pages[f] < 0 || pages[f] >= g->n_pages) return fail(PM_ERR_INVALID, "page %lld out of range", (long long)pages[f]);
+    if (pf[pages[f]] != PAGE_ABSENT) return fail(PM_ERR_INVALID, "page %lld listed twice", (long long)pages[f]);
+    pf[pages[f]] = (int32_t)f;
+  }
+  memcpy(s->init_pf, pf.data(), sizeof(int32_t) * g->n_pages);
+  for (int64_t f = 0; f < g->n_frames; f++) s->init_fp[f] = f < k ? (int32_t)pages[f] : -1;
+  s->prefilled = k;
+  return PM_OK;
+}

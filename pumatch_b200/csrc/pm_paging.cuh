@@ -1,0 +1,188 @@
+// pm_paging.cuh -- device side of the adjacency page cache (paged residency).
+//
+// Replaces the reference's GPU-side LRU package buffer and its fault
+// handshake (src/buffer.cu:197-261 get_neighbors_from_buffer, :581-628
+// lruAccess_bucket, :800-871 update_buffer, :1859-1936 add_vertex_block) and
+// the missing-branch tree (src/missing_tree.cu) with a design in which no
+// device thread ever waits for the host:
+//   * the adjacency array stays in pinned, mapped host memory; a page is a
+//     fixed power-of-two range of it; a device frame pool caches pages;
+//   * page_frame[page] is the device-resident page table (frame index, or
+//     ABSENT / LOADING / EVICTING);
+//   * a warp that finds a list resident pins its frame, re-checks the
+//     mapping and reads the frame; a list spanning several pages is gathered
+//     into the warp's arena when all its pages are resident;
+//   * otherwise the warp reads the list straight from host memory over the
+//     link (so every branch finishes where it started -- nothing is parked or
+//     lost, counts stay exact) and, for an absent page, claims a victim frame
+//     with a bounded CLOCK sweep (skipping pinned and referenced frames) and
+//     posts (page, frame) to a ring in mapped host memory;
+//   * a host service thread copies posted pages into their frames with
+//     cudaMemcpyAsync on a side stream and publishes each page by copying its
+//     page-table entry after the data (same stream, so the entry lands
+//     after the page).
+#pragma once
+
+#include "pm_device.cuh"
+
+namespace pm {
+
+enum : int32_t { PAGE_EVICTING = -3 };
+
+struct PageCounters {
+  unsigned long long hits, misses, zc_bytes, requests, evictions, dropped;
+};
+
+__device__ __forceinline__ int32_t ld_vol(const int32_t* p) { return *(const volatile int32_t*)p; }
+
+// Reserves one ring slot if the host has room; returns the slot or ~0ull.
+__device__ __forceinline__ unsigned long long ring_reserve(const DPaging& pg) {
+  for (int t = 0; t < 8; t++) {
+    const unsigned long long head = *(volatile unsigned long long*)pg.ring_head;
+    const unsigned long long done = *(volatile unsigned long long*)pg.host_tail;
+    if (head - done >= (unsigned long long)pg.ring_mask) return ~0ull;  // full
+    if (atomicCAS(pg.ring_head, head, head + 1) == head) return head;
+  }
+  return ~0ull;
+}
+
+__device__ __forceinline__ void ring_post(const DPaging& pg, unsigned long long slot, int32_t page, int32_t frame) {
+  pg.ring[slot & pg.ring_mask] = make_int2(page, frame);
+  __threadfence_system();
+  *(volatile unsigned long long*)&pg.ring_seq[slot & pg.ring_mask] = slot + 1;
+}
+
+// Lane 0 only.  Starts loading page p if it is absent: reserve a ring slot,
+// claim the page, find a frame (never-used frames first, then a bounded
+// CLOCK sweep), post the request.  Never waits for the host.
+static __device__ void request_page(const DPaging& pg, int32_t p, PageCounters& pc) {
+  if (ld_vol(&pg.page_frame[p]) != PAGE_ABSENT) return;
+  const unsigned long long slot = ring_reserve(pg);
+  if (slot == ~0ull) { pc.dropped++; return; }
+  if (atomicCAS(&pg.page_frame[p], PAGE_ABSENT, PAGE_LOADING) != PAGE_ABSENT) {
+    ring_post(pg, slot, -1, -1);  // someone else is loading it
+    return;
+  }
+  int32_t f = -1;
+  const unsigned long long k = atomicAdd(pg.next_free, 1ull);
+  if (k < (unsigned long long)pg.n_frames) {
+    f = (int32_t)k;
+  } else {
+    for (int t = 0; t < 4096 && f < 0; t++) {
+      const int32_t h = (int32_t)(atomicAdd(pg.clock_hand, 1ull) % (unsigned long long)pg.n_frames);
+      if (pg.frame_ref[h]) { pg.frame_ref[h] = 0; continue; }
+      if (ld_vol(&pg.frame_pin[h]) != 0) continue;
+      const int32_t q = ld_vol(&pg.frame_page[h]);
+      if (q < 0) continue;
+      if (atomicCAS(&pg.page_frame[q], h, PAGE_EVICTING) != h) continue;
+      __threadfence();
+      if (ld_vol(&pg.frame_pin[h]) != 0) {  // a reader pinned it meanwhile
+        atomicExch(&pg.page_frame[q], h);
+        continue;
+      }
+      atomicExch(&pg.page_frame[q], PAGE_ABSENT);
+      f = h;
+      pc.evictions++;
+    }
+  }
+  if (f < 0) {  // every frame busy: stay on the host-read path
+    atomicExch(&pg.page_frame[p], PAGE_ABSENT);
+    ring_post(pg, slot, -1, -1);
+    pc.dropped++;
+    return;
+  }
+  atomicExch(&pg.frame_page[f], p);
+  ring_post(pg, slot, p, f);
+  pc.requests++;
+}
+
+// Pins the frame holding page p if it is resident; returns the frame or -1.
+__device__ __forceinline__ int32_t try_pin(const DPaging& pg, int32_t p) {
+  const int32_t f = ld_vol(&pg.page_frame[p]);
+  if (f < 0) return -1;
+  atomicAdd(&pg.frame_pin[f], 1);
+  __threadfence();
+  if (ld_vol(&pg.page_frame[p]) != f) {
+    atomicSub(&pg.frame_pin[f], 1);
+    return -1;
+  }
+  pg.frame_ref[f] = 1;
+  return f;
+}
+
+struct ListRef {
+  const int32_t* p;
+  int len;
+  int32_t pinned;  // frame to unpin after use, or -1
+};
+
+// Most pages one list may span and still be gathered from frames; longer
+// lists are read from host memory.
+#define PM_MAX_LIST_PAGES 64
+
+// Resolves the adjacency list [b, b+len) of colidx for the whole warp.
+// gather: arena space for a multi-page list (>= len words); pins: per-warp
+// shared scratch of PM_MAX_LIST_PAGES frame indices.  Frames are remembered
+// from the pin, never re-read from the table (an evictor can hold an entry at
+// PAGE_EVICTING for a moment even while the frame is pinned).
+static __device__ ListRef paged_list(const DPaging& pg, uint64_t b, int len, int32_t* gather, int32_t* pins,
+                                     PageCounters& pc) {
+  const int lane = threadIdx.x & 31;
+  if (len == 0) return ListRef{pg.host_colidx + b, 0, -1};
+  const int sh = pg.page_shift;
+  const int32_t p0 = (int32_t)(b >> sh);
+  const int32_t p1 = (int32_t)((b + (uint64_t)len - 1) >> sh);
+  int mode = 1;  // 0 frame, 1 host read, 2 gathered
+  int32_t f0 = -1;
+  if (lane == 0) {
+    if (p0 == p1) {
+      f0 = try_pin(pg, p0);
+      if (f0 >= 0) mode = 0;
+      else request_page(pg, p0, pc);
+    } else if (p1 - p0 < PM_MAX_LIST_PAGES) {
+      int32_t k = p0;
+      for (; k <= p1; k++) {
+        const int32_t f = try_pin(pg, k);
+        if (f < 0) break;
+        pins[k - p0] = f;
+      }
+      if (k > p1) {
+        mode = 2;
+      } else {
+        for (int32_t j = p0; j < k; j++) atomicSub(&pg.frame_pin[pins[j - p0]], 1);
+        for (int32_t j = p0, posted = 0; j <= p1 && posted < 4; j++)
+          if (ld_vol(&pg.page_frame[j]) == PAGE_ABSENT) { request_page(pg, j, pc); posted++; }
+      }
+    }
+    if (mode == 1) { pc.misses++; pc.zc_bytes += 4ull * (unsigned long long)len; }
+    else pc.hits++;
+  }
+  mode = __shfl_sync(0xffffffffu, mode, 0);
+  f0 = __shfl_sync(0xffffffffu, f0, 0);
+  if (mode == 0) {
+    const uint64_t off = b & ((1ull << sh) - 1);
+    return ListRef{pg.frames + ((uint64_t)f0 << sh) + off, len, f0};
+  }
+  if (mode == 1) return ListRef{pg.host_colidx + b, len, -1};
+  // gather the pinned pages into the arena, then unpin them
+  __syncwarp();
+  const uint64_t e = b + (uint64_t)len;
+  for (int32_t k = p0; k <= p1; k++) {
+    const int32_t f = pins[k - p0];
+    const uint64_t s0 = max(b, (uint64_t)k << sh), s1 = min(e, ((uint64_t)k + 1) << sh);
+    const int32_t* src = pg.frames + ((uint64_t)f << sh) + (s0 - ((uint64_t)k << sh));
+    int32_t* dst = gather + (s0 - b);
+    for (uint64_t i = lane; i < s1 - s0; i += 32) dst[i] = __ldcg(src + i);
+  }
+  __syncwarp();
+  if (lane == 0)
+    for (int32_t k = p0; k <= p1; k++) atomicSub(&pg.frame_pin[pins[k - p0]], 1);
+  __syncwarp();
+  return ListRef{gather, len, -1};
+}
+
+__device__ __forceinline__ void unpin(const DPaging& pg, const ListRef& r) {
+  if (r.pinned >= 0 && (threadIdx.x & 31) == 0) atomicSub(&pg.frame_pin[r.pinned], 1);
+}
+
+}  // namespace pm
