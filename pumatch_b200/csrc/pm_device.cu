@@ -108,6 +108,10 @@ struct MatchArgs {
 enum { ST_SETOPS = 0, ST_BYTES = 1, ST_ROOTS = 2, ST_SPLITS = 3, ST_HITS = 4, ST_MISSES = 5,
        ST_ZC_BYTES = 6, ST_REQUESTS = 7, ST_EVICTIONS = 8, ST_DROPPED = 9 };
 
+#define PM_SB_MAX 512      // ints of a leaf batch's common operand kept in shared memory
+#define PM_LANE_MAX 96     // longest first operand one lane handles alone in a leaf batch
+#define PM_LEAF_BATCH 512  // candidates per leaf batch
+
 struct WarpState {
   int32_t path[8];
   int32_t iter[8];
@@ -118,6 +122,7 @@ struct WarpState {
   unsigned long long next_beat;  // setops value at which to bump the heartbeat
   unsigned long long t_start;    // %globaltimer at kernel entry (ns)
   int32_t pins[PM_MAX_LIST_PAGES];  // paged mode: frames pinned for a gather
+  int32_t sb[PM_SB_MAX];            // leaf batches: shared copy of the common operand
 };
 
 // Per-warp work counters (registers; flushed once at kernel exit).
@@ -226,7 +231,8 @@ __device__ int run_slot(const MatchArgs& a, const DPlan& P, WarpState& S, int32_
   const bool fresh_unl = (!LABELED && kind == SLOT_FRESH);
   if (fresh_unl && T && scan > T) scan = T;  // first pass keeps A's prefix
   int cnt = 0;
-  if (!last && top + scan > a.slot_words) {
+  // the slot holds at most the first T survivors
+  if (!last && top + ((T && scan > T) ? T : scan) > a.slot_words) {
     w.err |= DEV_ARENA_OVERFLOW;
     scan = 0;
   }
@@ -279,6 +285,149 @@ __device__ __forceinline__ int run_level(const MatchArgs& a, const DPlan& P, War
   return top;
 }
 
+// First index of sorted A[0,len) whose element is >= x (one lane).
+__device__ __forceinline__ int lane_lower_bound(const int32_t* A, int len, int x) {
+  int lo = 0, hi = len;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (A[mid] < x) lo = mid + 1; else hi = mid;
+  }
+  return lo;
+}
+
+// The last level for the candidates [b, e) of level L's main slot (each is
+// v_{n-2} in turn): one lane per candidate, counting only.  Same set
+// operations and counts as run_slot(last) per candidate, organised so that
+// short operands cost one lane each:
+//   * unlabeled fresh sets and copies are counted with binary searches (the
+//     prefix below the bound, minus path vertices found in it);
+//   * intersections merge the candidate's list with the common second operand
+//     (staged in shared memory when it fits), galloping through it;
+//   * a labeled copy is the same for every candidate: counted once;
+//   * candidates whose first operand is longer than PM_LANE_MAX go back to the
+//     warp-cooperative run_slot.
+template <bool LABELED>
+__device__ unsigned long long leaf_batch(const MatchArgs& a, const DPlan& P, WarpState& S, int32_t* arena, int L,
+                                         int b, int e, Work& w) {
+  const int lane = lane_id();
+  const int s = P.last_slot;
+  const int kind = P.kind[s];
+  const int Lf = L + 1;
+  const int32_t* cand = arena + S.off[P.level_begin[L]];
+  const int par = P.parent[s];
+  const int32_t* B = arena + S.off[par];  // intersect: second operand; copy: first operand
+  const int lenB = S.size[par];
+  const uint32_t mask = P.slot_labels[s];
+  const int T = a.T;
+  unsigned long long cnt_warp = 0;  // uniform across lanes
+  if (LABELED && kind == SLOT_COPY) {
+    int k = 0;
+    for (int i = lane; i < lenB; i += 32) k += (mask >> a.labels[B[i]]) & 1u;
+    for (int o = 16; o; o >>= 1) k += __shfl_xor_sync(FULL, k, o);
+    if (T && k > T) k = T;
+    const unsigned long long m = (unsigned long long)(e - b);
+    w.setops += m;
+    w.bytes += m * (4ull * (unsigned long long)(lenB + k) + (unsigned long long)lenB);
+    return m * (unsigned long long)k;
+  }
+  // symmetry-breaking bound: bits 0..L are common, bit L+1 is the candidate
+  int common_ub = INT_MAX;
+  bool self_ub = false;
+  if (!LABELED && P.partial[s]) {
+    for (int j = 0; j <= L; j++)
+      if (P.partial[s] & (1u << j)) common_ub = min(common_ub, S.path[j]);
+    self_ub = (P.partial[s] >> Lf) & 1u;
+  }
+  const int32_t* Bs = B;
+  if (kind == SLOT_INTERSECT && lenB <= PM_SB_MAX) {
+    for (int i = lane; i < lenB; i += 32) S.sb[i] = B[i];
+    __syncwarp();
+    Bs = S.sb;
+  }
+  unsigned long long cnt = 0, bytes = 0, ops = 0;  // per lane
+  for (int base = b; base < e; base += 32) {
+    const int i = base + lane;
+    const bool mine = i < e;
+    const int c = mine ? cand[i] : 0;
+    bool deferred = false;
+    if (mine) {
+      const int ub = self_ub ? min(common_ub, c) : common_ub;
+      if (kind == SLOT_COPY) {  // unlabeled: A = parent slot minus the candidate
+        const int lenA = (ub == INT_MAX) ? lenB : lane_lower_bound(B, lenB, ub);
+        const int pos = lane_lower_bound(B, lenA, c);
+        int k = lenA - ((pos < lenA && B[pos] == c) ? 1 : 0);
+        if (T && k > T) k = T;
+        cnt += k;
+        bytes += 4ull * (unsigned long long)(lenA + k);
+        ops++;
+      } else {
+        const uint64_t rb = a.rowptr[c];
+        const int deg = (int)(a.rowptr[c + 1] - rb);
+        const int32_t* A = a.colidx + rb;
+        const int lenA = (ub == INT_MAX) ? deg : lane_lower_bound(A, deg, ub);
+        if (!LABELED && kind == SLOT_FRESH) {
+          // first min(lenA, T) elements, minus the path vertices among them
+          const int lim = (T && lenA > T) ? T : lenA;
+          int k = lim;
+          for (int j = 0; j <= L; j++) {
+            const int pj = S.path[j];
+            const int pos = lane_lower_bound(A, lim, pj);
+            k -= (pos < lim && A[pos] == pj) ? 1 : 0;
+          }
+          cnt += k;
+          bytes += 4ull * (unsigned long long)(lenA + k);
+          ops++;
+        } else if (lenA > PM_LANE_MAX) {
+          deferred = true;
+        } else if (kind == SLOT_FRESH) {  // labeled: label filter only
+          int k = 0;
+          for (int x = 0; x < lenA; x++) k += (mask >> a.labels[A[x]]) & 1u;
+          if (T && k > T) k = T;
+          cnt += k;
+          bytes += 4ull * (unsigned long long)(lenA + k) + (unsigned long long)lenA;
+          ops++;
+        } else {  // intersection with the common operand
+          int k = 0, p = 0;
+          for (int x = 0; x < lenA && p < lenB; x++) {
+            const int v = A[x];
+            int lo = p, step = 1;
+            while (lo + step < lenB && Bs[lo + step] < v) { lo += step; step <<= 1; }
+            int hi = min(lo + step + 1, lenB);
+            while (lo < hi) {
+              const int mid = (lo + hi) >> 1;
+              if (Bs[mid] < v) lo = mid + 1; else hi = mid;
+            }
+            p = lo;
+            if (p < lenB && Bs[p] == v && (!LABELED || ((mask >> a.labels[v]) & 1u))) k++;
+          }
+          if (T && k > T) k = T;
+          cnt += k;
+          bytes += 4ull * (unsigned long long)(lenA + lenB + k) + (LABELED ? (unsigned long long)lenA : 0ull);
+          ops++;
+        }
+      }
+    }
+    // long first operands: the warp takes them one by one
+    unsigned dm = __ballot_sync(FULL, deferred);
+    while (dm) {
+      const int src = __ffs(dm) - 1;
+      dm &= dm - 1;
+      const int cc = __shfl_sync(FULL, c, src);
+      if (lane == 0) S.path[Lf] = cc;
+      __syncwarp();
+      cnt_warp += (unsigned long long)run_slot<LABELED, false>(a, P, S, arena, Lf, s, S.top[Lf], true, w);
+    }
+  }
+  for (int o = 16; o; o >>= 1) {
+    cnt += __shfl_xor_sync(FULL, cnt, o);
+    bytes += __shfl_xor_sync(FULL, bytes, o);
+    ops += __shfl_xor_sync(FULL, ops, o);
+  }
+  w.setops += ops;
+  w.bytes += bytes;
+  return cnt + cnt_warp;
+}
+
 // Depth-first enumeration below a root edge, over level-1 candidates
 // [b1, e1) (e1 < 0: all).  Restates match() (src/gpu_match.cu:855-1047)
 // without deferral: every branch is finished where it starts.
@@ -291,7 +440,13 @@ __device__ unsigned long long dfs_root(const MatchArgs& a, const DPlan& P, WarpS
   if (lane == 0) { S.path[0] = v0; S.path[1] = v1; S.top[1] = 0; }
   __syncwarp();
   if (n == 3) return (unsigned long long)run_slot<LABELED, PAGED>(a, P, S, arena, 1, P.level_begin[1], 0, true, w);
-  run_level<LABELED, PAGED>(a, P, S, arena, 1, w);
+  {
+    // a donated range recomputes level 1 of its root: that repeat is not
+    // part of the reference's work, so it is kept out of the counters
+    const unsigned long long so = w.setops, by = w.bytes, rd = w.reads;
+    run_level<LABELED, PAGED>(a, P, S, arena, 1, w);
+    if (b1 > 0 || e1 >= 0) { w.setops = so; w.bytes = by; w.reads = rd; }
+  }
   if (w.err) return 0;
   unsigned long long cnt = 0;
   const int m1 = P.level_begin[1];
@@ -343,7 +498,13 @@ __device__ unsigned long long dfs_root(const MatchArgs& a, const DPlan& P, WarpS
         return 0;
       }
     }
-    if (it < iend) {
+    if (!PAGED && it < iend && L + 1 == n - 2) {
+      const int e2 = min(iend, it + PM_LEAF_BATCH);
+      cnt += leaf_batch<LABELED>(a, P, S, arena, L, it, e2, w);
+      if (lane == 0) S.iter[L] = e2;
+      __syncwarp();
+      if (w.err) return 0;
+    } else if (it < iend) {
       const int v = arena[S.off[m] + it];
       if (lane == 0) { S.iter[L] = it + 1; S.path[L + 1] = v; }
       __syncwarp();
@@ -403,8 +564,10 @@ __device__ bool take_donation(const MatchArgs& a, int4& item) {
   return got != 0;
 }
 
-template <bool LABELED, bool PAGED>
-__global__ void __launch_bounds__(512) match_kernel(MatchArgs a) {
+// MINB = 4: 64 registers, four 256-thread blocks per SM (more warps in flight,
+// some spills); MINB = 1: up to 128 registers, no spills, fewer warps.
+template <bool LABELED, bool PAGED, int MINB>
+__global__ void __launch_bounds__(MINB == 1 ? 512 : 256, MINB) match_kernel(MatchArgs a) {
   extern __shared__ WarpState smem_state[];
   const int lane = lane_id();
   const int wib = threadIdx.x >> 5;
@@ -1024,8 +1187,14 @@ static pm_status setup_launch(pm_ctx* c, const pm_graph* g, const pm_plan* const
   // launch geometry: persistent, occupancy-limited
   L->threads = wpb * 32;
   L->smem = sizeof(WarpState) * wpb;
-  L->kfn = L->labeled ? (L->paged ? match_kernel<true, true> : match_kernel<true, false>)
-                      : (L->paged ? match_kernel<false, true> : match_kernel<false, false>);
+  if (o.low_occupancy) {
+    L->kfn = L->labeled ? (L->paged ? match_kernel<true, true, 1> : match_kernel<true, false, 1>)
+                        : (L->paged ? match_kernel<false, true, 1> : match_kernel<false, false, 1>);
+  } else {
+    if (wpb > 8) return fail(PM_ERR_INVALID, "warps_per_block 16 needs low_occupancy (256-thread blocks otherwise)");
+    L->kfn = L->labeled ? (L->paged ? match_kernel<true, true, 4> : match_kernel<true, false, 4>)
+                        : (L->paged ? match_kernel<false, true, 4> : match_kernel<false, false, 4>);
+  }
   int per_sm = 0;
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, L->kfn, L->threads, L->smem));
   if (o.blocks_per_sm > 0) per_sm = std::min(per_sm, o.blocks_per_sm);

@@ -3,7 +3,8 @@ its counts (tests/golden/ref_gpu_counts.json).
 
 Needs a GPU and the binaries built by `make -C oracle ref` (oracle/_ref/
 ref_test_{labeled,unlabeled}[_t16]: the reference's untouched sources with
-LABELED / GRAPH_DEGREE selected by -include shims).  Reads only files under
+LABELED / GRAPH_DEGREE selected by -include shims, device code built with -G
+as the reference's Makefile does).  Reads only files under
 this repository.
 
     python tests/golden/make_ref_gpu_counts.py --out gpurun_out/ref_gpu_counts.json
@@ -60,8 +61,11 @@ def main():
                 pfile = os.path.join(tmp, pname + ".g")
                 open(pfile, "w").write(pats[pname])
                 t0 = time.time()
-                r = subprocess.run([exe, os.path.join(HERE, "graphs", gname), pfile], capture_output=True,
-                                   text=True, cwd=tmp, timeout=args.timeout)
+                for attempt in range(2):  # the reference's host threads crash now and then (SIGSEGV)
+                    r = subprocess.run([exe, os.path.join(HERE, "graphs", gname), pfile], capture_output=True,
+                                       text=True, cwd=tmp, timeout=args.timeout)
+                    if r.returncode == 0:
+                        break
                 if r.returncode != 0:
                     print(f"FAILED {binary} {gname} {pname}: rc={r.returncode}\n{r.stderr[-2000:]}", flush=True)
                     continue

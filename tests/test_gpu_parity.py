@@ -129,17 +129,20 @@ def test_gpu_batched_launch(ctx):
     assert single == got
 
 
-@pytest.mark.parametrize("wpb", [1, 2, 4, 8])
+@pytest.mark.parametrize("wpb", [1, 2, 4, 8, 16])
 @pytest.mark.parametrize("chunk", [1, 7, 64])
 def test_gpu_launch_shapes(ctx, wpb, chunk):
     hg = host_graph("cl400", False)
     g = dev_graph("cl400", False)
-    text = PATTERNS["house"]
-    want, _ = oracle_count(hg, text, False)
-    for split in (-1, 1, 8):
-        got, st = ctx.match(g, [pm.PatternPreprocessor(text=text, labeled=False)], warps_per_block=wpb,
-                            chunk=chunk, split_level1=split)
-        assert got[0] == want, (wpb, chunk, split)
+    for pname in ("house", "clique5", "path5", "star5"):
+        text = PATTERNS[pname]
+        want, st = oracle_count(hg, text, False)
+        for split in (-1, 1, 8):
+            for low in ((True,) if wpb == 16 else (False, True)):
+                got, gst = ctx.match(g, [pm.PatternPreprocessor(text=text, labeled=False)], warps_per_block=wpb,
+                                     chunk=chunk, split_level1=split, low_occupancy=low)
+                assert got[0] == want, (pname, wpb, chunk, split, low)
+                assert gst["set_ops"] == st["set_ops"] and gst["alg_bytes"] == st["alg_bytes"]
 
 
 def test_gpu_shards_and_root_ranges(ctx):
