@@ -228,7 +228,7 @@ def run_ours(args, workload):
     stream = torch.cuda.ExternalStream(ctx.stream_ptr, device=torch.device("cuda", local))
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")  # > 126 MB L2
     shard = dict(shard_rank=rank, shard_count=world) if world > 1 else {}
-    run_kw = dict(timeout_ms=args.timeout_s * 1000, low_occupancy=args.low_occupancy, **shard)
+    run_kw = dict(timeout_ms=args.timeout_s * 1000, high_occupancy=args.high_occupancy, **shard)
     if args.root_limit > 0:
         run_kw.update(root_begin=0, root_end=args.root_limit)
 
@@ -315,7 +315,7 @@ def run_ours(args, workload):
             "data": "synthetic",
             "config": {"workload": workload, "graph": w["graph"], "labeled": w["labeled"],
                        "patterns": [p for p, _ in texts], "counts": counts_total,
-                       "kernel_variant": "low_occupancy" if args.low_occupancy else "default",
+                       "kernel_variant": "high_occupancy" if args.high_occupancy else "default",
                        "root_limit": args.root_limit or None,
                        "roots": int(st["n_roots"]), "set_ops_per_step": set_ops // args.steps,
                        "l2": "flushed between timed steps (256 MB write)",
@@ -352,7 +352,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--timeout-s", type=int, default=120, help="hard device-side limit per launch")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--low-occupancy", action="store_true", help="kernel variant with <=128 registers")
+    ap.add_argument("--high-occupancy", action="store_true", help="kernel variant capped at 64 registers")
     ap.add_argument("--root-limit", type=int, default=0, help="profile a prefix of the root list only")
     args = ap.parse_args()
     if args.impl == "reference":

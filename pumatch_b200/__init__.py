@@ -62,7 +62,7 @@ class RunOpts(C.Structure):
                 ("chunk", C.c_int32), ("split_level1", C.c_int32), ("shard_rank", C.c_int32),
                 ("shard_count", C.c_int32), ("use_graph", C.c_int32), ("timeout_ms", C.c_int32),
                 ("root_begin", C.c_int64), ("root_end", C.c_int64), ("cold_cache", C.c_int32),
-                ("low_occupancy", C.c_int32), ("reserved_", C.c_int32 * 2),
+                ("high_occupancy", C.c_int32), ("reserved_", C.c_int32 * 2),
                 ("root_counts", C.c_void_p), ("root_cost", C.c_void_p), ("root_order", C.c_void_p),
                 ("root_reads", C.c_void_p)]
 
@@ -404,7 +404,7 @@ class Context:
               shard_rank: int = 0, shard_count: int = 0, root_begin: int = -1, root_end: int = -1,
               root_counts_ptr: int = 0, root_cost_ptr: int = 0, root_order_ptr: int = 0, root_reads_ptr: int = 0,
               use_graph: bool = False, timeout_ms: int = 0, cold_cache: bool = False,
-              low_occupancy: bool = False):
+              high_occupancy: bool = False):
         """Runs all patterns in one launch; returns (counts list, stats dict)."""
         o = RunOpts()
         lib().pm_run_opts_default(C.byref(o))
@@ -413,7 +413,7 @@ class Context:
         o.root_begin, o.root_end, o.use_graph = root_begin, root_end, int(use_graph)
         o.timeout_ms = timeout_ms
         o.cold_cache = int(cold_cache)
-        o.low_occupancy = int(low_occupancy)
+        o.high_occupancy = int(high_occupancy)
         o.root_counts = root_counts_ptr or None
         o.root_cost = root_cost_ptr or None
         o.root_order = root_order_ptr or None

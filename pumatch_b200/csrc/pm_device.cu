@@ -91,8 +91,8 @@ struct MatchArgs {
   float* root_cost;
   float* root_reads;
   const int32_t* root_order;
-  // donation ring: items (plan, root, begin, end) -- level-1 ranges
-  int4* don_items;
+  // donation ring: items (plan, root, level, begin, end, path[2..level])
+  int4* don_items;                // 3 int4 per slot
   unsigned long long* don_head;   // next slot to fill
   unsigned long long* don_ready;  // per slot: sequence number + 1 when filled
   unsigned int don_mask;
@@ -120,6 +120,7 @@ struct WarpState {
   int32_t off[16];
   int32_t size[16];
   unsigned long long next_beat;  // setops value at which to bump the heartbeat
+  unsigned long long next_split; // setops value at which to look for idle warps
   unsigned long long t_start;    // %globaltimer at kernel entry (ns)
   int32_t pins[PM_MAX_LIST_PAGES];  // paged mode: frames pinned for a gather
   int32_t sb[PM_SB_MAX];            // leaf batches: shared copy of the common operand
@@ -428,64 +429,76 @@ __device__ unsigned long long leaf_batch(const MatchArgs& a, const DPlan& P, War
   return cnt + cnt_warp;
 }
 
-// Depth-first enumeration below a root edge, over level-1 candidates
-// [b1, e1) (e1 < 0: all).  Restates match() (src/gpu_match.cu:855-1047)
-// without deferral: every branch is finished where it starts.
+// A donated piece of a DFS: candidates [begin, end) of level `level`'s main
+// slot under the path root(v0, v1), path[2..level].
+struct Donation {
+  int plan, root, level, begin, end;
+  int path[7];  // path[2..level] used
+};
+
+// Hands the upper half of the shallowest level range that is long enough to
+// the donation ring, when some warps are idle and fewer pieces are queued
+// than idle warps.  Lane 0 decides.
+__device__ __forceinline__ void maybe_donate(const MatchArgs& a, WarpState& S, int L0, int L, int plan_id,
+                                             int root_id) {
+  const int lane = lane_id();
+  if (lane == 0) {
+    const unsigned int act = *((volatile unsigned int*)a.active);
+    const unsigned long long head = *((volatile unsigned long long*)a.don_head);
+    const unsigned long long tail = *((volatile unsigned long long*)a.don_tail);
+    if (act < a.total_warps && head - tail < (unsigned long long)(a.total_warps - act) &&
+        head - tail < (unsigned long long)a.don_mask) {
+      for (int k = L0; k <= L; k++) {
+        const int it = S.iter[k], iend = S.iend[k];
+        if (iend - it < max(a.split_min, 2)) continue;
+        const int mid = it + (iend - it) / 2;  // it < mid < iend
+        const unsigned long long slot = atomicAdd(a.don_head, 1ull);
+        int4* dst = a.don_items + 3 * (slot & a.don_mask);
+        dst[0] = make_int4(plan_id, root_id, k, mid);
+        dst[1] = make_int4(iend, S.path[2], S.path[3], S.path[4]);
+        dst[2] = make_int4(S.path[5], S.path[6], 0, 0);
+        __threadfence();
+        atomicExch(&a.don_ready[slot & a.don_mask], slot + 1);
+        atomicAdd(&a.stats[ST_SPLITS], 1ull);
+        S.iend[k] = mid;
+        break;
+      }
+    }
+  }
+  __syncwarp();
+}
+
+// Depth-first enumeration below a fixed path prefix.  path[0..L0] must be
+// set; levels 1..L0 are computed here (for a donated piece this repeats the
+// donor's work and is kept out of the counters), then candidates [b, e) of
+// level L0's main slot (e < 0: all) are enumerated to the last level.
+// Restates match() (src/gpu_match.cu:855-1047) without deferral: every
+// branch is finished where it starts.
 template <bool LABELED, bool PAGED>
-__device__ unsigned long long dfs_root(const MatchArgs& a, const DPlan& P, WarpState& S, int32_t* arena,
-                                       int v0, int v1, int b1, int e1, bool may_split, int plan_id,
-                                       int root_id, Work& w) {
+__device__ unsigned long long dfs_from(const MatchArgs& a, const DPlan& P, WarpState& S, int32_t* arena, int L0,
+                                       int b, int e, bool counted_prefix, int plan_id, int root_id, Work& w) {
   const int lane = lane_id();
   const int n = P.nnodes;
-  if (lane == 0) { S.path[0] = v0; S.path[1] = v1; S.top[1] = 0; }
+  if (lane == 0) S.top[1] = 0;
   __syncwarp();
   if (n == 3) return (unsigned long long)run_slot<LABELED, PAGED>(a, P, S, arena, 1, P.level_begin[1], 0, true, w);
   {
-    // a donated range recomputes level 1 of its root: that repeat is not
-    // part of the reference's work, so it is kept out of the counters
     const unsigned long long so = w.setops, by = w.bytes, rd = w.reads;
-    run_level<LABELED, PAGED>(a, P, S, arena, 1, w);
-    if (b1 > 0 || e1 >= 0) { w.setops = so; w.bytes = by; w.reads = rd; }
+    for (int k = 1; k <= L0 && !w.err; k++) run_level<LABELED, PAGED>(a, P, S, arena, k, w);
+    if (!counted_prefix) { w.setops = so; w.bytes = by; w.reads = rd; }
   }
   if (w.err) return 0;
   unsigned long long cnt = 0;
-  const int m1 = P.level_begin[1];
-  int end1 = S.size[m1];
-  if (e1 >= 0 && e1 < end1) end1 = e1;
-  if (lane == 0) { S.iter[1] = b1; S.iend[1] = end1; }
-  __syncwarp();
-  int L = 1;
+  {
+    int end0 = S.size[P.level_begin[L0]];
+    if (e >= 0 && e < end0) end0 = e;
+    if (lane == 0) { S.iter[L0] = b; S.iend[L0] = end0; }
+    __syncwarp();
+  }
+  int L = L0;
   while (true) {
-    const int m = P.level_begin[L];
-    const int it = S.iter[L];
-    int iend = (L == 1) ? S.iend[1] : S.size[m];
-    // donate the upper half of a long level-1 range when warps are idle
-    if (L == 1 && may_split && a.split_min > 0 && iend - it >= max(a.split_min, 2)) {
-      int gave = 0, newend = iend;
-      if (lane == 0) {
-        const unsigned int act = *((volatile unsigned int*)a.active);
-        const unsigned long long head = *((volatile unsigned long long*)a.don_head);
-        const unsigned long long tail = *((volatile unsigned long long*)a.don_tail);
-        // only while some warps idle and fewer ranges are queued than idle warps
-        if (act < a.total_warps && head - tail < (unsigned long long)(a.total_warps - act)) {
-          const unsigned long long slot = atomicAdd(a.don_head, 1ull);
-          const int mid = it + (iend - it) / 2;  // it < mid < iend
-          a.don_items[slot & a.don_mask] = make_int4(plan_id, root_id, mid, iend);
-          __threadfence();
-          atomicExch(&a.don_ready[slot & a.don_mask], slot + 1);
-          atomicAdd(&a.stats[ST_SPLITS], 1ull);
-          gave = 1;
-          newend = mid;
-          S.iend[1] = mid;
-        }
-      }
-      gave = __shfl_sync(FULL, gave, 0);
-      newend = __shfl_sync(FULL, newend, 0);
-      if (gave) iend = newend;
-      __syncwarp();
-    }
-    // liveness signal for idle warps and the kernel-wide deadline, checked
-    // once per ~1024 set operations
+    // liveness signal for idle warps and the launch-wide deadline, then the
+    // periodic look for idle warps to hand work to
     if (w.setops >= S.next_beat) {
       int late = 0;
       if (lane == 0) {
@@ -498,6 +511,13 @@ __device__ unsigned long long dfs_root(const MatchArgs& a, const DPlan& P, WarpS
         return 0;
       }
     }
+    if (a.split_min > 0 && w.setops >= S.next_split) {
+      if (lane == 0) S.next_split = w.setops + 64;
+      maybe_donate(a, S, L0, L, plan_id, root_id);
+    }
+    const int m = P.level_begin[L];
+    const int it = S.iter[L];
+    const int iend = S.iend[L];
     if (!PAGED && it < iend && L + 1 == n - 2) {
       const int e2 = min(iend, it + PM_LEAF_BATCH);
       cnt += leaf_batch<LABELED>(a, P, S, arena, L, it, e2, w);
@@ -513,24 +533,24 @@ __device__ unsigned long long dfs_root(const MatchArgs& a, const DPlan& P, WarpS
       } else {
         L++;
         run_level<LABELED, PAGED>(a, P, S, arena, L, w);
-        if (lane == 0) S.iter[L] = 0;
+        if (lane == 0) { S.iter[L] = 0; S.iend[L] = S.size[P.level_begin[L]]; }
         __syncwarp();
       }
       if (w.err) return 0;
     } else {
       L--;
-      if (L < 1) break;
+      if (L < L0) break;
     }
   }
   return cnt;
 }
 
-// Takes one donated level-1 range if any is queued.  The caller is counted
-// as active before it claims, so "no active warp and nothing queued" is a
-// safe exit test for everyone.  Returns false if nothing was taken.
-__device__ bool take_donation(const MatchArgs& a, int4& item) {
+// Takes one donated piece if any is queued.  The caller is counted as active
+// before it claims, so "no active warp and nothing queued" is a safe exit
+// test for everyone.  Returns false if nothing was taken.
+__device__ bool take_donation(const MatchArgs& a, Donation& d) {
   int got = 0;
-  int4 it = make_int4(0, 0, 0, 0);
+  int v[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
   if (lane_id() == 0) {
     const unsigned long long tail = *((volatile unsigned long long*)a.don_tail);
     const unsigned long long head = *((volatile unsigned long long*)a.don_head);
@@ -545,8 +565,8 @@ __device__ bool take_donation(const MatchArgs& a, int4& item) {
         }
         if (got) {
           __threadfence();
-          const volatile int* src = (const volatile int*)&a.don_items[tail & a.don_mask];
-          it = make_int4(src[0], src[1], src[2], src[3]);
+          const volatile int* src = (const volatile int*)(a.don_items + 3 * (tail & a.don_mask));
+          for (int i = 0; i < 12; i++) v[i] = src[i];
         } else {
           atomicOr(a.status, (unsigned)DEV_TIMEOUT);
           atomicSub(a.active, 1u);
@@ -557,10 +577,21 @@ __device__ bool take_donation(const MatchArgs& a, int4& item) {
     }
   }
   got = __shfl_sync(FULL, got, 0);
-  item.x = __shfl_sync(FULL, it.x, 0);
-  item.y = __shfl_sync(FULL, it.y, 0);
-  item.z = __shfl_sync(FULL, it.z, 0);
-  item.w = __shfl_sync(FULL, it.w, 0);
+  int u[12];
+#pragma unroll
+  for (int i = 0; i < 12; i++) u[i] = __shfl_sync(FULL, v[i], 0);
+  d.plan = u[0];
+  d.root = u[1];
+  d.level = u[2];
+  d.begin = u[3];
+  d.end = u[4];
+  d.path[0] = 0;
+  d.path[1] = 0;
+  d.path[2] = u[5];
+  d.path[3] = u[6];
+  d.path[4] = u[7];
+  d.path[5] = u[8];
+  d.path[6] = u[9];
   return got != 0;
 }
 
@@ -572,7 +603,7 @@ __global__ void __launch_bounds__(MINB == 1 ? 512 : 256, MINB) match_kernel(Matc
   const int lane = lane_id();
   const int wib = threadIdx.x >> 5;
   WarpState& S = smem_state[wib];
-  if (lane == 0) { S.next_beat = 0; S.t_start = global_ns(); }
+  if (lane == 0) { S.next_beat = 0; S.next_split = 0; S.t_start = global_ns(); }
   __syncwarp();
   const long long gw = (long long)blockIdx.x * (blockDim.x >> 5) + wib;
   int32_t* arena = a.arena + gw * a.arena_words;
@@ -603,8 +634,9 @@ __global__ void __launch_bounds__(MINB == 1 ? 512 : 256, MINB) match_kernel(Matc
       const long long rid = a.root_order ? (long long)a.root_order[r] : r;
       const int2 e = P.roots[rid];
       const unsigned long long b0 = w.bytes, r0 = w.reads;
-      const unsigned long long c0 =
-          dfs_root<LABELED, PAGED>(a, P, S, arena, e.x, e.y, 0, -1, true, p, (int)rid, w);
+      if (lane == 0) { S.path[0] = e.x; S.path[1] = e.y; }
+      __syncwarp();
+      const unsigned long long c0 = dfs_from<LABELED, PAGED>(a, P, S, arena, 1, 0, -1, true, p, (int)rid, w);
       local += c0;
       roots++;
       if (lane == 0 && p == 0) {
@@ -622,19 +654,25 @@ __global__ void __launch_bounds__(MINB == 1 ? 512 : 256, MINB) match_kernel(Matc
   __syncwarp();
   unsigned long long last_beat = 0, last_change = global_ns();
   while (!w.err) {
-    int4 item;
+    Donation item;
     if (take_donation(a, item)) {
-      const DPlan& P = c_plans[item.x];
-      const int2 e = P.roots[item.y];
-      const unsigned long long b0 = w.bytes, r0 = w.reads;
-      const unsigned long long c0 =
-          dfs_root<LABELED, PAGED>(a, P, S, arena, e.x, e.y, item.z, item.w, true, item.x, item.y, w);
+      const DPlan& P = c_plans[item.plan];
+      const int2 e = P.roots[item.root];
       if (lane == 0) {
-        if (c0) atomicAdd(&a.counts[item.x], c0);
-        if (item.x == 0) {
-          if (a.root_counts) atomicAdd(&a.root_counts[item.y], c0);
-          if (a.root_cost) atomicAdd(&a.root_cost[item.y], (float)(w.bytes - b0));
-          if (a.root_reads) atomicAdd(&a.root_reads[item.y], (float)(w.reads - r0));
+        S.path[0] = e.x;
+        S.path[1] = e.y;
+        for (int k = 2; k <= item.level; k++) S.path[k] = item.path[k];
+      }
+      __syncwarp();
+      const unsigned long long b0 = w.bytes, r0 = w.reads;
+      const unsigned long long c0 = dfs_from<LABELED, PAGED>(a, P, S, arena, item.level, item.begin, item.end,
+                                                             false, item.plan, item.root, w);
+      if (lane == 0) {
+        if (c0) atomicAdd(&a.counts[item.plan], c0);
+        if (item.plan == 0) {
+          if (a.root_counts) atomicAdd(&a.root_counts[item.root], c0);
+          if (a.root_cost) atomicAdd(&a.root_cost[item.root], (float)(w.bytes - b0));
+          if (a.root_reads) atomicAdd(&a.root_reads[item.root], (float)(w.reads - r0));
         }
         __threadfence();
         atomicSub(a.active, 1u);
@@ -1127,7 +1165,7 @@ struct Launch {
   unsigned int active0 = 0;  // initial active-warp count (host staging)
 };
 
-static constexpr unsigned kDonSlots = 1u << 16;
+static constexpr unsigned kDonSlots = 1u << 15;
 static constexpr int kCtlRead = 32 + 32 + 16 + 1;  // cursors, counts, stats, status word
 
 // Validates the plans and options, builds the root lists into *roots,
@@ -1187,11 +1225,11 @@ static pm_status setup_launch(pm_ctx* c, const pm_graph* g, const pm_plan* const
   // launch geometry: persistent, occupancy-limited
   L->threads = wpb * 32;
   L->smem = sizeof(WarpState) * wpb;
-  if (o.low_occupancy) {
+  if (!o.high_occupancy) {
     L->kfn = L->labeled ? (L->paged ? match_kernel<true, true, 1> : match_kernel<true, false, 1>)
                         : (L->paged ? match_kernel<false, true, 1> : match_kernel<false, false, 1>);
   } else {
-    if (wpb > 8) return fail(PM_ERR_INVALID, "warps_per_block 16 needs low_occupancy (256-thread blocks otherwise)");
+    if (wpb > 8) return fail(PM_ERR_INVALID, "warps_per_block 16 is not available with high_occupancy");
     L->kfn = L->labeled ? (L->paged ? match_kernel<true, true, 4> : match_kernel<true, false, 4>)
                         : (L->paged ? match_kernel<false, true, 4> : match_kernel<false, false, 4>);
   }
@@ -1213,7 +1251,7 @@ static pm_status setup_launch(pm_ctx* c, const pm_graph* g, const pm_plan* const
   if (st != PM_OK) return st;
   // control block: cursors[32] counts[32] stats[16] status/active head tail
   // heartbeat, donation ready[] and items[]
-  L->ctl_words = 32 + 32 + 16 + 8 + kDonSlots + 2 * kDonSlots;
+  L->ctl_words = 32 + 32 + 16 + 8 + kDonSlots + 6 * kDonSlots;
   st = ensure((void**)ctl, ctl_bytes, L->ctl_words * 8);
   if (st != PM_OK) return st;
 
@@ -1240,7 +1278,7 @@ static pm_status setup_launch(pm_ctx* c, const pm_graph* g, const pm_plan* const
   a.don_tail = w; w += 1;
   a.heartbeat = w; w += 5;
   a.don_ready = w; w += kDonSlots;
-  a.don_items = (int4*)w; w += 2 * kDonSlots;
+  a.don_items = (int4*)w; w += 6 * kDonSlots;
   a.don_mask = kDonSlots - 1;
   a.total_warps = (unsigned int)L->warps;
   a.arena = *arena;

@@ -68,7 +68,8 @@ static __device__ void request_page(const DPaging& pg, int32_t p, PageCounters& 
   if (k < (unsigned long long)pg.n_frames) {
     f = (int32_t)k;
   } else {
-    for (int t = 0; t < 4096 && f < 0; t++) {
+    const int sweep = (int)min((int64_t)4096, 2 * pg.n_frames + 8);  // bounded CLOCK sweep
+    for (int t = 0; t < sweep && f < 0; t++) {
       const int32_t h = (int32_t)(atomicAdd(pg.clock_hand, 1ull) % (unsigned long long)pg.n_frames);
       if (pg.frame_ref[h]) { pg.frame_ref[h] = 0; continue; }
       if (ld_vol(&pg.frame_pin[h]) != 0) continue;

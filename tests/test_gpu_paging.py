@@ -15,7 +15,7 @@ _cache = {}
 def workload():
     if "w" not in _cache:
         # hubs well above one 4 KiB page (1024 ids) so multi-page lists occur
-        hg = pm.gen_chung_lu(30000, 200000, gamma=2.1, i0=5.0, max_w=3000.0, seed=41)
+        hg = pm.gen_chung_lu(8000, 40000, gamma=2.1, i0=3.0, max_w=2500.0, seed=41)
         lab = pm.gen_labels(hg.n, 4, seed=42)
         _cache["w"] = pm.HostGraph(hg.rowptr, hg.colidx, lab)
     return _cache["w"]

@@ -138,10 +138,10 @@ def test_gpu_launch_shapes(ctx, wpb, chunk):
         text = PATTERNS[pname]
         want, st = oracle_count(hg, text, False)
         for split in (-1, 1, 8):
-            for low in ((True,) if wpb == 16 else (False, True)):
+            for high in ((False,) if wpb == 16 else (False, True)):
                 got, gst = ctx.match(g, [pm.PatternPreprocessor(text=text, labeled=False)], warps_per_block=wpb,
-                                     chunk=chunk, split_level1=split, low_occupancy=low)
-                assert got[0] == want, (pname, wpb, chunk, split, low)
+                                     chunk=chunk, split_level1=split, high_occupancy=high)
+                assert got[0] == want, (pname, wpb, chunk, split, high)
                 assert gst["set_ops"] == st["set_ops"] and gst["alg_bytes"] == st["alg_bytes"]
 
 
