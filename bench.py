@@ -37,35 +37,67 @@ from pumatch_b200 import patterns as P  # noqa: E402
 
 # name -> definition.  Graph sizes/seeds follow the configuration each one
 # stands in for; the reasons for each stand-in are in DESIGN.md.
+_CL100K = dict(kind="chung_lu", n=100_000, m=1_000_000, gamma=2.1, i0=10.0, max_w=5000.0, seed=1)
+_RMAT1M = dict(kind="rmat", n=1 << 20, m=16 << 20, a=0.57, b=0.19, c=0.19, seed=2)
+_RMAT128K = dict(kind="rmat", n=1 << 17, m=16 << 17, a=0.57, b=0.19, c=0.19, seed=2)
 WORKLOADS = {
     # Chung-Lu 100K vertices / 1M edges, gamma 2.1, expected degrees capped
     # at 5,000, unlabeled, in HBM; one 7-vertex query: the 7-clique.
-    "chunglu100k_k7": dict(graph=dict(kind="chung_lu", n=100_000, m=1_000_000, gamma=2.1, i0=10.0,
-                                      max_w=5000.0, seed=1),
-                           labeled=False, n_labels=0, patterns=[("K7", P.clique(7))]),
+    "chunglu100k_k7": dict(graph=_CL100K, labeled=False, n_labels=0, patterns=[("K7", P.clique(7))]),
     # the same graph with 16 uniform labels and the 7-cycle (labeled semantics)
-    "chunglu100k_c7_lab16": dict(graph=dict(kind="chung_lu", n=100_000, m=1_000_000, gamma=2.1, i0=10.0,
-                                            max_w=5000.0, seed=1),
-                                 labeled=True, n_labels=16, label_seed=102, pattern_label_seed=202,
+    "chunglu100k_c7_lab16": dict(graph=_CL100K, labeled=True, n_labels=16, label_seed=102, pattern_label_seed=202,
                                  patterns=[("C7", P.cycle(7))]),
+    # the K7 query with the adjacency in host memory and a frame pool of 1/8
+    # of it (the reference's out-of-core mode on the C1 graph)
+    "chunglu100k_k7_paged": dict(graph=_CL100K, labeled=False, n_labels=0, patterns=[("K7", P.clique(7))],
+                                 paged=dict(frame_fraction=0.125, page_bytes=16 << 10)),
+    # R-MAT (a,b,c = .57,.19,.19) 1M vertices / 16M edges, 32 labels, the
+    # 5-cycle plus 2-vertex pendant path, in HBM and paged (pool = 1/4)
+    "rmat1m_c5t2_lab32": dict(graph=_RMAT1M, labeled=True, n_labels=32, label_seed=102, pattern_label_seed=202,
+                              patterns=[("C5t2", P.cycle_tail(5, 2))]),
+    "rmat1m_c5t2_lab32_paged": dict(graph=_RMAT1M, labeled=True, n_labels=32, label_seed=102,
+                                    pattern_label_seed=202, patterns=[("C5t2", P.cycle_tail(5, 2))],
+                                    paged=dict(frame_fraction=0.25, page_bytes=64 << 10)),
+    # twenty seeded 4-7-vertex patterns in one persistent launch
+    "rmat128k_batch20_lab32": dict(graph=_RMAT128K, labeled=True, n_labels=32, label_seed=102, batch_seed=303),
+    # learned-scheduler comparison (--learned): trained on seeds 11, 12, 13
+    "rmat128k_c5t2_lab32_paged": dict(graph=_RMAT128K, labeled=True, n_labels=32, label_seed=102,
+                                      pattern_label_seed=202, patterns=[("C5t2", P.cycle_tail(5, 2))],
+                                      paged=dict(frame_fraction=0.25, page_bytes=16 << 10)),
 }
 DEFAULT_WORKLOAD = "chunglu100k_k7"
 
 
-def build_workload(name):
-    w = WORKLOADS[name]
-    g = w["graph"]
+def make_graph(g, seed=None):
+    seed = g["seed"] if seed is None else seed
     if g["kind"] == "chung_lu":
-        hg = pm.gen_chung_lu(g["n"], g["m"], gamma=g["gamma"], i0=g["i0"], max_w=g["max_w"], seed=g["seed"])
-    else:
-        hg = pm.gen_rmat(g["n"], g["m"], a=g.get("a", 0.57), b=g.get("b", 0.19), c=g.get("c", 0.19), seed=g["seed"])
+        return pm.gen_chung_lu(g["n"], g["m"], gamma=g["gamma"], i0=g["i0"], max_w=g["max_w"], seed=seed)
+    return pm.gen_rmat(g["n"], g["m"], a=g["a"], b=g["b"], c=g["c"], seed=seed)
+
+
+def build_workload(name, graph_seed=None):
+    w = WORKLOADS[name]
+    hg = make_graph(w["graph"], graph_seed)
     if w["labeled"]:
-        hg = pm.HostGraph(hg.rowptr, hg.colidx, pm.gen_labels(hg.n, w["n_labels"], seed=w["label_seed"]))
-    texts = []
-    for i, (pname, (k, edges)) in enumerate(w["patterns"]):
-        labs = P.seeded_labels(k, w["n_labels"], w["pattern_label_seed"] + i) if w["labeled"] else None
-        texts.append((pname, P.to_g(k, edges, labs)))
+        ls = w["label_seed"] if graph_seed is None else w["label_seed"] + 1000 * graph_seed
+        hg = pm.HostGraph(hg.rowptr, hg.colidx, pm.gen_labels(hg.n, w["n_labels"], seed=ls))
+    if "batch_seed" in w:
+        texts = P.batch_of_20(seed=w["batch_seed"], n_labels=w["n_labels"])
+    else:
+        texts = []
+        for i, (pname, (k, edges)) in enumerate(w["patterns"]):
+            labs = P.seeded_labels(k, w["n_labels"], w["pattern_label_seed"] + i) if w["labeled"] else None
+            texts.append((pname, P.to_g(k, edges, labs)))
     return w, hg, texts
+
+
+def place_graph(w, hg, device):
+    pg = w.get("paged")
+    if not pg:
+        return pm.GraphPreprocessor.from_host(hg, labeled=w["labeled"], device=device)
+    pool = max(pg["page_bytes"], int(hg.colidx.nbytes * pg["frame_fraction"]) // pg["page_bytes"] * pg["page_bytes"])
+    return pm.GraphPreprocessor.from_host(hg, labeled=w["labeled"], device=device, paged=True,
+                                          page_bytes=pg["page_bytes"], frame_pool_bytes=pool)
 
 
 def dist_env():
@@ -224,7 +256,7 @@ def run_ours(args, workload):
     labeled = w["labeled"]
     plans = [pm.PatternPreprocessor(text=t, labeled=labeled) for _, t in texts]
     ctx = pm.Context(local)
-    graph = pm.GraphPreprocessor.from_host(hg, labeled=labeled, device=local)
+    graph = place_graph(w, hg, local)
     stream = torch.cuda.ExternalStream(ctx.stream_ptr, device=torch.device("cuda", local))
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")  # > 126 MB L2
     shard = dict(shard_rank=rank, shard_count=world) if world > 1 else {}
@@ -287,7 +319,7 @@ def run_ours(args, workload):
         if dist:
             dist.barrier()
         t0 = time.perf_counter()
-        g2 = pm.GraphPreprocessor.from_host(hg, labeled=labeled, device=local)
+        g2 = place_graph(w, hg, local)
         c2, _ = ctx.match(g2, plans, **run_kw)
         g2.close()
         torch.cuda.synchronize()
@@ -343,6 +375,74 @@ def run_ours(args, workload):
         dist.destroy_process_group()
 
 
+def run_learned(args, workload):
+    """Plain vs learned (heavy-first root order + learned page residency) on
+    the workload's graph, the model trained on plain runs over three other
+    seeds of the same generator.  Counts must be identical."""
+    import torch
+
+    from pumatch_b200 import learn
+    torch.cuda.set_device(0)
+    ctx = pm.Context(0)
+    w, hg, texts = build_workload(workload)
+    if len(texts) != 1:
+        raise SystemExit("--learned needs a single-pattern workload")
+    labeled = w["labeled"]
+    xs, ts = [], []
+    t0 = time.time()
+    for seed in (11, 12, 13):
+        _, hgs, _ = build_workload(workload, graph_seed=seed)
+        gs = pm.GraphPreprocessor.from_host(hgs, labeled=labeled)
+        ps = pm.PatternPreprocessor(text=texts[0][1], labeled=labeled)
+        _, _, cost, reads = learn.plain_costs(ctx, gs, ps, timeout_ms=args.timeout_s * 1000)
+        xs.append(learn.root_features(ctx, gs, ps))
+        ts.append(learn.targets(cost, reads))
+        gs.close()
+    x, t = torch.cat(xs), torch.cat(ts)
+    model = learn.CostModel(0, seed=1)
+    hist = model.fit(x, t, epochs=args.learn_epochs, batch=4096, lr=3e-3)
+    train_s = time.time() - t0
+    p = pm.PatternPreprocessor(text=texts[0][1], labeled=labeled)
+    g = place_graph(w, hg, 0)
+    xe = learn.root_features(ctx, g, p)
+    pred = model.predict(xe)
+    count, st, cost, reads = learn.plain_costs(ctx, g, p, timeout_ms=args.timeout_s * 1000)
+    te = learn.targets(cost, reads)
+    mae = (pred - te).abs().mean(0).tolist()
+    base = (te - t.mean(0)).abs().mean(0).tolist()
+    order = learn.heavy_first_order(pred)
+    if w.get("paged"):
+        info = g.info()
+        roots = ctx.roots(g, p)
+        score = learn.page_scores(hg.rowptr, roots, torch.expm1(pred[:, 1].clamp_min(0)).cpu().numpy(),
+                                  w["paged"]["page_bytes"] // 4, info["n_pages"])
+    kw = dict(timeout_ms=args.timeout_s * 1000, cold_cache=bool(w.get("paged")))
+    res = {}
+    for mode in ("plain", "learned"):
+        if mode == "learned" and w.get("paged"):
+            import numpy as np
+            g.set_resident_pages(np.argsort(-score)[:info["n_frames"]])
+        extra = dict(root_order_ptr=order.data_ptr()) if mode == "learned" else {}
+        if mode == "learned" and w.get("paged"):
+            extra["cold_cache"] = False
+        times, stats = [], None
+        for k in range(args.warmup + args.steps):
+            c, stt = ctx.match(g, [p], **kw, **extra)
+            assert c[0] == count, (mode, c, count)
+            if k >= args.warmup:
+                times.append(stt["kernel_ms"])
+                stats = stt
+        res[mode] = {"kernel_ms": statistics.median(times), "page_misses": stats["page_misses"],
+                     "pages_loaded": stats["pages_loaded"], "zero_copy_bytes": stats["zero_copy_bytes"],
+                     "splits": stats["splits"]}
+    line = {"metric": "query_ms_learned_vs_plain", "workload": workload, "count": count,
+            "plain": res["plain"], "learned": res["learned"],
+            "speedup": res["plain"]["kernel_ms"] / res["learned"]["kernel_ms"],
+            "prediction_mae_log": mae, "constant_predictor_mae_log": base, "train_loss": [hist[0], hist[-1]],
+            "train_s": train_s, "train_roots": int(x.shape[0]), "eval_roots": int(xe.shape[0])}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -354,8 +454,12 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--high-occupancy", action="store_true", help="kernel variant capped at 64 registers")
     ap.add_argument("--root-limit", type=int, default=0, help="profile a prefix of the root list only")
+    ap.add_argument("--learned", action="store_true", help="plain vs learned scheduling on the workload")
+    ap.add_argument("--learn-epochs", type=int, default=20)
     args = ap.parse_args()
-    if args.impl == "reference":
+    if args.learned:
+        run_learned(args, args.workload)
+    elif args.impl == "reference":
         run_reference(args, args.workload)
     else:
         run_ours(args, args.workload)

@@ -72,6 +72,10 @@ struct MatchArgs {
   const uint64_t* rowptr;
   const int32_t* colidx;        // HBM residency
   const uint8_t* labels;
+  const int32_t* colidx_lab;    // label-grouped lists (labeled, HBM) or null
+  const int32_t* lab_off;
+  int32_t nl1;
+  int32_t pad1;
   int32_t n;
   int32_t nplans;
   int32_t T;
@@ -182,6 +186,14 @@ __device__ __forceinline__ ListRef adj(const MatchArgs& a, WarpState& S, int v, 
   return paged_list(a.pg, b, len, gather, S.pins, w.pc);
 }
 
+// The label-l part of v's list (labeled graphs in HBM), in id order.
+__device__ __forceinline__ ListRef adj_label(const MatchArgs& a, int v, int l) {
+  const uint64_t b = a.rowptr[v];
+  const int32_t* o = a.lab_off + (int64_t)v * a.nl1;
+  const int s0 = o[l], s1 = o[l + 1];
+  return ListRef{a.colidx_lab + b + s0, s1 - s0, -1};
+}
+
 // ---------------------------------------------------------------------
 // One slot of level L for the warp's current path.  Restates compute_set
 // (src/gpu_match.cu:238-319) with the operand choice of extend
@@ -197,7 +209,18 @@ __device__ int run_slot(const MatchArgs& a, const DPlan& P, WarpState& S, int32_
   int32_t* gatherA = arena + a.slot_words;
   int32_t* gatherB = gatherA + a.maxdeg;
   ListRef RA, RB{nullptr, 0, -1};
-  if (kind != SLOT_COPY) {
+  // one-label masks read only that label's part of an adjacency list: same
+  // survivors in the same order, no label gathers (accounting still charges
+  // the whole list, as the reference scans it)
+  const uint32_t mask0 = P.slot_labels[s];
+  const bool by_label = LABELED && !PAGED && a.colidx_lab && __popc(mask0) == 1 && (kind != SLOT_COPY || L == 1);
+  int full_len = -1;  // length of the whole list when by_label
+  if (by_label) {
+    const int v = (kind != SLOT_COPY) ? vL : S.path[0];
+    full_len = (int)(a.rowptr[v + 1] - a.rowptr[v]);
+    RA = adj_label(a, v, __ffs(mask0) - 1);
+    w.reads++;
+  } else if (kind != SLOT_COPY) {
     RA = adj<PAGED>(a, S, vL, gatherA, w);
   } else if (L > 1) {
     RA = ListRef{arena + S.off[P.parent[s]], S.size[P.parent[s]], -1};
@@ -246,7 +269,7 @@ __device__ int run_slot(const MatchArgs& a, const DPlan& P, WarpState& S, int32_
     bool keep = valid;
     if (kind == SLOT_INTERSECT && keep) keep = bsearch_in<PAGED>(B, lenB, x);
     if (LABELED) {
-      if (keep) keep = (mask >> a.labels[x]) & 1u;
+      if (keep && !by_label) keep = (mask >> a.labels[x]) & 1u;
     } else if (kind == SLOT_COPY) {
       keep = keep && x != vL;
     } else if (kind == SLOT_FRESH) {
@@ -266,9 +289,77 @@ __device__ int run_slot(const MatchArgs& a, const DPlan& P, WarpState& S, int32_
     unpin(a.pg, RB);
   }
   if (T && cnt > T) cnt = T;
+  const int alenA = by_label ? full_len : lenA;
   w.setops++;
-  w.bytes += 4ull * (unsigned long long)(lenA + lenB + cnt) + (LABELED ? (unsigned long long)lenA : 0ull);
+  w.bytes += 4ull * (unsigned long long)(alenA + lenB + cnt) + (LABELED ? (unsigned long long)alenA : 0ull);
   return cnt;
+}
+
+// Bound of slot s at level L from the partial order: the smallest (main
+// slot) or largest (helper slot) constrained path vertex; INT_MAX if none.
+template <bool LABELED>
+__device__ __forceinline__ int slot_bound(const DPlan& P, const WarpState& S, int L, int s) {
+  if (LABELED || !P.partial[s]) return INT_MAX;
+  const bool is_main = (s == P.level_begin[L]);
+  long long ub = is_main ? INT_MAX : -1;
+  for (int j = 0; j <= L; j++) {
+    if (!(P.partial[s] & (1u << j))) continue;
+    const long long v = S.path[j];
+    if (is_main) { if (v <= ub) ub = v; }
+    else if (ub < v) ub = v;
+  }
+  return ub == -1 ? INT_MAX : (int)ub;
+}
+
+// A slot equal to, or a prefix of, a slot already computed at this level:
+// no scan, only the reference's accounting for the set operation it stands
+// for (its first operand's length below its bound, its result length).
+template <bool LABELED, bool PAGED>
+__device__ void alias_slot(const MatchArgs& a, const DPlan& P, WarpState& S, int32_t* arena, int L, int s, Work& w) {
+  const int t = P.alias[s];
+  const int ub = slot_bound<LABELED>(P, S, L, s);
+  int size = S.size[t];
+  if (P.alias_prefix[s] && ub != INT_MAX) size = warp_lower_bound<false>(arena + S.off[t], size, ub);
+  // first operand length as the reference would scan it
+  const int kind = P.kind[s];
+  int lenA, lenB = 0;
+  if (kind != SLOT_COPY) {
+    const int v = S.path[L];
+    lenA = (int)(a.rowptr[v + 1] - a.rowptr[v]);
+    if (ub != INT_MAX) {
+      if (PAGED) {
+        ListRef r = adj<PAGED>(a, S, v, arena + a.slot_words, w);
+        lenA = warp_lower_bound<PAGED>(r.p, r.len, ub);
+        __syncwarp();
+        unpin(a.pg, r);
+      } else {
+        lenA = warp_lower_bound<false>(a.colidx + a.rowptr[v], lenA, ub);
+      }
+    }
+  } else if (L > 1) {
+    lenA = S.size[P.parent[s]];
+    if (ub != INT_MAX) lenA = warp_lower_bound<false>(arena + S.off[P.parent[s]], lenA, ub);
+  } else {
+    const int v = S.path[0];
+    lenA = (int)(a.rowptr[v + 1] - a.rowptr[v]);
+    if (ub != INT_MAX) {
+      if (PAGED) {
+        ListRef r = adj<PAGED>(a, S, v, arena + a.slot_words, w);
+        lenA = warp_lower_bound<PAGED>(r.p, r.len, ub);
+        __syncwarp();
+        unpin(a.pg, r);
+      } else {
+        lenA = warp_lower_bound<false>(a.colidx + a.rowptr[v], lenA, ub);
+      }
+    }
+  }
+  if (kind == SLOT_INTERSECT) {
+    if (L > 1) lenB = S.size[P.parent[s]];
+    else lenB = (int)(a.rowptr[S.path[0] + 1] - a.rowptr[S.path[0]]);
+  }
+  w.setops++;
+  w.bytes += 4ull * (unsigned long long)(lenA + lenB + size) + (LABELED ? (unsigned long long)lenA : 0ull);
+  if (lane_id() == 0) { S.off[s] = S.off[t]; S.size[s] = size; }
 }
 
 // Computes every slot of level L; returns the arena top after them.
@@ -277,9 +368,15 @@ __device__ __forceinline__ int run_level(const MatchArgs& a, const DPlan& P, War
                                          int L, Work& w) {
   int top = S.top[L];
   for (int s = P.level_begin[L]; s < P.level_begin[L + 1]; s++) {
+    if (P.alias[s] >= 0) continue;
     const int sz = run_slot<LABELED, PAGED>(a, P, S, arena, L, s, top, false, w);
     if (lane_id() == 0) { S.off[s] = top; S.size[s] = sz; }
     top += sz;
+  }
+  __syncwarp();
+  for (int s = P.level_begin[L]; s < P.level_begin[L + 1]; s++) {
+    if (P.alias[s] < 0) continue;
+    alias_slot<LABELED, PAGED>(a, P, S, arena, L, s, w);
   }
   if (lane_id() == 0) S.top[L + 1] = top;
   __syncwarp();
@@ -366,7 +463,41 @@ __device__ unsigned long long leaf_batch(const MatchArgs& a, const DPlan& P, War
         const int deg = (int)(a.rowptr[c + 1] - rb);
         const int32_t* A = a.colidx + rb;
         const int lenA = (ub == INT_MAX) ? deg : lane_lower_bound(A, deg, ub);
-        if (!LABELED && kind == SLOT_FRESH) {
+        if (LABELED && a.colidx_lab && __popc(mask) == 1) {
+          // the label-l part of the list: a fresh set is its length, an
+          // intersection merges only it
+          const int32_t* o = a.lab_off + (int64_t)c * a.nl1;
+          const int l = __ffs(mask) - 1;
+          const int32_t* Al = a.colidx_lab + rb + o[l];
+          const int lenl = o[l + 1] - o[l];
+          int k = 0;
+          if (kind == SLOT_FRESH) {
+            k = lenl;
+          } else if (lenl > PM_LANE_MAX) {
+            deferred = true;
+          } else {
+            int p = 0;
+            for (int x = 0; x < lenl && p < lenB; x++) {
+              const int v = Al[x];
+              int lo = p, step = 1;
+              while (lo + step < lenB && Bs[lo + step] < v) { lo += step; step <<= 1; }
+              int hi = min(lo + step + 1, lenB);
+              while (lo < hi) {
+                const int mid = (lo + hi) >> 1;
+                if (Bs[mid] < v) lo = mid + 1; else hi = mid;
+              }
+              p = lo;
+              k += (p < lenB && Bs[p] == v) ? 1 : 0;
+            }
+          }
+          if (!deferred) {
+            if (T && k > T) k = T;
+            cnt += k;
+            bytes += 4ull * (unsigned long long)(deg + (kind == SLOT_INTERSECT ? lenB : 0) + k) +
+                     (unsigned long long)deg;
+            ops++;
+          }
+        } else if (!LABELED && kind == SLOT_FRESH) {
           // first min(lenA, T) elements, minus the path vertices among them
           const int lim = (T && lenA > T) ? T : lenA;
           int k = lim;
@@ -743,6 +874,54 @@ __global__ void maxnbrdeg_kernel(const uint64_t* rowptr, const int32_t* colidx, 
   }
 }
 
+// Regroups each list by label, keeping id order within a label (a stable
+// partition): one warp per vertex, ranks from __match_any_sync.
+__global__ void label_group_kernel(const uint64_t* rowptr, const int32_t* colidx, const uint8_t* labels, int64_t n,
+                                   int nl1, int32_t* out, int32_t* off) {
+  __shared__ int base_s[16][33];
+  const int lane = lane_id();
+  const int wib = threadIdx.x >> 5;
+  int* base = base_s[wib];
+  const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
+  for (long long v = (long long)blockIdx.x * (blockDim.x >> 5) + wib; v < n; v += warps) {
+    const uint64_t b = rowptr[v], e = rowptr[v + 1];
+    // per-label counts: lane l counts label l
+    int mine = 0;
+    for (uint64_t i0 = b; i0 < e; i0 += 32) {
+      const uint64_t i = i0 + lane;
+      const int lb = i < e ? labels[colidx[i]] : -1;
+      for (int l = 0; l < nl1 - 1; l++) {
+        const unsigned bal = __ballot_sync(FULL, lb == l);
+        if (lane == l) mine += __popc(bal);
+      }
+    }
+    // exclusive scan over labels
+    int incl = mine;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(FULL, incl, o);
+      if (lane >= o) incl += t;
+    }
+    const int excl = incl - mine;
+    if (lane < nl1 - 1) {
+      off[v * nl1 + lane] = excl;
+      base[lane] = excl;
+    }
+    if (lane == 0) off[v * nl1 + nl1 - 1] = (int)(e - b);  // up to 32 labels: entry 32 needs its own store
+    __syncwarp();
+    for (uint64_t i0 = b; i0 < e; i0 += 32) {
+      const uint64_t i = i0 + lane;
+      const bool valid = i < e;
+      const int x = valid ? colidx[i] : 0;
+      const int lb = valid ? (int)labels[x] : 32 + lane;  // invalid lanes match only themselves
+      const unsigned same = __match_any_sync(FULL, lb);
+      if (valid) out[b + base[lb] + __popc(same & lanemask_lt())] = x;
+      __syncwarp();
+      if (valid && (same & lanemask_lt()) == 0) base[lb] += __popc(same);
+      __syncwarp();
+    }
+  }
+}
+
 struct RootFilter {
   int labeled;
   int need_gt;   // unlabeled with partial[0]==1: keep r > c only
@@ -821,11 +1000,33 @@ DPlan to_dplan(const Plan& p) {
   d.labeled = p.labeled;
   d.last_slot = p.level_begin[p.nnodes - 2];
   for (int i = 0; i <= PM_MAX_PAT; i++) d.level_begin[i] = p.level_begin[i];
+  for (int s = 0; s < 16; s++) d.alias[s] = -1;
   for (int s = 0; s < p.nslots; s++) {
     d.slot_labels[s] = p.slot_labels[s];
     d.partial[s] = p.partial[s];
     d.kind[s] = (uint8_t)slot_kind(p.set_ops[s]);
     d.parent[s] = (uint8_t)slot_parent(p.set_ops[s]);
+  }
+  // Slots of one level with the same operation, operands, labels and partial
+  // order differ only in how their bound combines the constrained path
+  // vertices: the main slot takes the smallest, helpers the largest.  A
+  // helper equal to an earlier helper is that helper; the main slot is the
+  // prefix of such a helper below its own (smaller) bound -- also under
+  // truncation, since both keep their first survivors in the same order.
+  for (int L = 1; L + 2 < p.nnodes; L++) {
+    const int b = p.level_begin[L], e = p.level_begin[L + 1];
+    for (int i = b + 1; i <= e; i++) {
+      const int s = (i == e) ? b : i;  // helpers first, the main slot last
+      for (int t = b + 1; t < e; t++) {
+        if (t == s || (s != b && t >= s)) continue;
+        if (p.set_ops[s] != p.set_ops[t] || p.slot_labels[s] != p.slot_labels[t] || p.partial[s] != p.partial[t])
+          continue;
+        if (d.alias[t] >= 0) continue;  // alias a computed slot only
+        d.alias[s] = (int8_t)t;
+        d.alias_prefix[s] = (s == b) ? 1 : 0;
+        break;
+      }
+    }
   }
   return d;
 }
@@ -857,6 +1058,7 @@ namespace pm {
 // mapped host memory).
 pm_status compute_maxnbrdeg(pm_graph* g, const int32_t* colidx) {
   if (g->n > 0) {
+    (void)cudaGetLastError();  // drop a stale error from an earlier call
     maxnbrdeg_kernel<<<2048, 256>>>(g->d_rowptr, colidx, g->n, g->d_maxnbrdeg);
     CK(cudaGetLastError());
     CK(cudaDeviceSynchronize());
@@ -870,7 +1072,19 @@ static pm_status graph_finish(pm_graph* g) {
   CK(cudaMalloc(&g->d_maxnbrdeg, sizeof(int32_t) * std::max<int64_t>(g->n, 1)));
   g->device_bytes += sizeof(int32_t) * g->n;
   if (g->n > 0 && g->residency == PM_RESIDENT_HBM) {
+    (void)cudaGetLastError();  // drop a stale error from an earlier call
     maxnbrdeg_kernel<<<2048, 256>>>(g->d_rowptr, g->d_colidx, g->n, g->d_maxnbrdeg);
+    CK(cudaGetLastError());
+    CK(cudaDeviceSynchronize());
+  }
+  if (g->labeled && g->residency == PM_RESIDENT_HBM && g->n > 0) {
+    g->nl1 = (g->nlabels > 0 ? g->nlabels : 32) + 1;
+    CK(cudaMalloc(&g->d_colidx_lab, sizeof(int32_t) * std::max<int64_t>(g->nadj, 1)));
+    CK(cudaMalloc(&g->d_lab_off, sizeof(int32_t) * (size_t)g->n * g->nl1));
+    g->device_bytes += sizeof(int32_t) * ((size_t)g->nadj + (size_t)g->n * g->nl1);
+    (void)cudaGetLastError();  // drop a stale error from an earlier call
+    label_group_kernel<<<2048, 256>>>(g->d_rowptr, g->d_colidx, g->d_labels, g->n, g->nl1, g->d_colidx_lab,
+                                      g->d_lab_off);
     CK(cudaGetLastError());
     CK(cudaDeviceSynchronize());
   }
@@ -1015,6 +1229,8 @@ extern "C" void pm_graph_close(pm_graph* g) {
     free_dev(g->d_labels);
   }
   free_dev(g->d_maxnbrdeg);
+  free_dev(g->d_colidx_lab);
+  free_dev(g->d_lab_off);
   paged_release(g);
   delete g;
 }
@@ -1078,6 +1294,7 @@ static pm_status build_roots(pm_ctx* c, const pm_graph* g, const Plan& p, size_t
   }
   const RootFilter f = to_filter(p);
   const int32_t* colidx = g->residency == PM_RESIDENT_HBM ? g->d_colidx : g->h_colidx_dev;
+  (void)cudaGetLastError();  // drop a stale error from an earlier call
   roots_kernel<false><<<4 * c->nsm, 256, 0, c->stream>>>(g->d_rowptr, colidx, g->d_labels, g->d_maxnbrdeg, n, f,
                                                           c->d_vcount, nullptr, nullptr);
   CK(cudaGetLastError());
@@ -1104,6 +1321,7 @@ static pm_status build_roots(pm_ctx* c, const pm_graph* g, const Plan& p, size_t
     *roots_buf = nr;
     *roots_bytes = want + want / 4;
   }
+  (void)cudaGetLastError();  // drop a stale error from an earlier call
   roots_kernel<true><<<4 * c->nsm, 256, 0, c->stream>>>(g->d_rowptr, colidx, g->d_labels, g->d_maxnbrdeg, n, f,
                                                          nullptr, c->d_voff, *roots_buf + offset_roots);
   CK(cudaGetLastError());
@@ -1260,6 +1478,9 @@ static pm_status setup_launch(pm_ctx* c, const pm_graph* g, const pm_plan* const
   a.rowptr = g->d_rowptr;
   a.colidx = g->d_colidx;
   a.labels = g->d_labels;
+  a.colidx_lab = g->d_colidx_lab;
+  a.lab_off = g->d_lab_off;
+  a.nl1 = g->nl1;
   a.n = (int32_t)g->n;
   a.nplans = nplans;
   a.T = T;
@@ -1306,10 +1527,11 @@ static pm_status enqueue_launch(pm_ctx* c, Launch& L, const DPlan* dp_src, const
   CK(cudaMemcpyToSymbolAsync(c_plans, dp_src, sizeof(DPlan) * L.nplans, 0, cudaMemcpyHostToDevice, c->stream));
   CK(cudaMemsetAsync(L.a.cursors, 0, L.ctl_words * 8, c->stream));
   CK(cudaMemcpyAsync(L.a.active, active_src, sizeof(unsigned int), cudaMemcpyHostToDevice, c->stream));
-  CK(cudaEventRecord(eb, c->stream));
+  if (eb) CK(cudaEventRecord(eb, c->stream));
+  (void)cudaGetLastError();  // drop a stale error from an earlier call
   L.kfn<<<L.blocks, L.threads, L.smem, c->stream>>>(L.a);
   CK(cudaGetLastError());
-  CK(cudaEventRecord(ee, c->stream));
+  if (ee) CK(cudaEventRecord(ee, c->stream));
   CK(cudaMemcpyAsync(host_ctl, L.a.cursors, sizeof(unsigned long long) * kCtlRead, cudaMemcpyDeviceToHost,
                      c->stream));
   return PM_OK;
@@ -1455,7 +1677,8 @@ extern "C" pm_status pm_query_prepare(pm_ctx* c, const pm_graph* g, const pm_pla
   CK(cudaEventCreate(&q->eb));
   CK(cudaEventCreate(&q->ee));
   CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-  pm_status est = enqueue_launch(c, q->L, q->h_dp, q->h_active, q->h_ctl, q->eb, q->ee);
+  // timing events stay outside the graph (recorded around each replay)
+  pm_status est = enqueue_launch(c, q->L, q->h_dp, q->h_active, q->h_ctl, nullptr, nullptr);
   cudaError_t cerr = cudaStreamEndCapture(c->stream, &q->graph);
   if (est != PM_OK) return est;
   CK(cerr);
@@ -1475,7 +1698,9 @@ extern "C" pm_status pm_query_run(pm_query* q, uint64_t* counts_out, pm_stats* s
   }
   pm_stats pst;
   pm_status st = run_launch(c, q->g, q->L, [&]() -> pm_status {
+    CK(cudaEventRecord(q->eb, c->stream));
     CK(cudaGraphLaunch(q->exec, c->stream));
+    CK(cudaEventRecord(q->ee, c->stream));
     return PM_OK;
   }, &pst);
   if (st != PM_OK) return st;

@@ -30,6 +30,10 @@ struct DPlan {
   uint32_t partial[16];
   uint8_t kind[16];               // SlotKind
   uint8_t parent[16];
+  int8_t alias[16];               // -1, or a slot of the same level with the
+                                  // same operation whose result contains this one
+  uint8_t alias_prefix[16];       // 1: this slot is the alias's prefix below
+                                  // this slot's own bound; 0: equal sets
   const int2* roots;              // (v0, v1) root edges, reference order
   int64_t nroots;
 };
@@ -76,6 +80,12 @@ struct pm_graph {
   int32_t* d_colidx = nullptr;   // HBM residency only
   uint8_t* d_labels = nullptr;
   int32_t* d_maxnbrdeg = nullptr;
+  // labeled graphs in HBM: each list regrouped by label (id order kept within
+  // a label) and per-vertex label offsets, so a one-label candidate set is a
+  // contiguous sub-range
+  int32_t* d_colidx_lab = nullptr;
+  int32_t* d_lab_off = nullptr;    // [n][nl1]: start of label l within v's list; [n][nl1-1] = deg
+  int32_t nl1 = 0;
   uint64_t device_bytes = 0;
   // paged residency (pm_paging.cu)
   int32_t* h_colidx = nullptr;     // pinned, mapped copy of the adjacency array

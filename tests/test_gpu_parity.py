@@ -42,7 +42,7 @@ def dev_graph(name, labeled):
     return _cache[key]
 
 
-def oracle_count(hg, text, labeled, truncate=0, threads=4):
+def oracle_count(hg, text, labeled, truncate=0, threads=os.cpu_count()):
     g = orc.Graph(hg.rowptr, hg.colidx, hg.labels if labeled else None)
     p = orc.plan(text, labeled)
     r = orc.roots(g, p)
@@ -78,6 +78,8 @@ def test_gpu_counts_match_oracle(ctx, gname, labeled):
     hg = host_graph(gname, labeled)
     g = dev_graph(gname, labeled)
     for pname in COUNT_PATTERNS:
+        if not labeled and pname.startswith("cycle5_tail2"):
+            continue  # minutes of oracle time unlabeled; covered labeled and on the small graphs
         text = PATTERNS[pname]
         want, st = oracle_count(hg, text, labeled)
         got, gst = ctx.match(g, [pm.PatternPreprocessor(text=text, labeled=labeled)])
