@@ -289,6 +289,42 @@ pm_status pm_mlp_train_step(pm_mlp* m, const float* d_x, const float* d_t, int64
 pm_status pm_mlp_get_weights(pm_mlp* m, float* host_out);
 pm_status pm_mlp_set_weights(pm_mlp* m, const float* host_in);
 
+/* ------------------------------------------------------------------ */
+/* Allocation-free matching (no counterpart in the reference)           */
+/* ------------------------------------------------------------------ */
+
+/* Bytes of the file-scope device scratch pm_match_static works in.  Every
+ * GPU that loads this library holds it from module load until exit. */
+#define PM_STATIC_SCRATCH_BYTES (64ull << 20)
+
+/* pm_match for callers that cannot allocate device memory (it has no
+ * counterpart in the reference, whose driver allocates everything up front,
+ * test.cu:59-154): code running in a
+ * stream callback or another library's allocator-locked region, a service
+ * whose device memory is budgeted and pooled elsewhere, or a framework that
+ * owns the allocator.  It calls no cudaMalloc/cudaFree and no allocating
+ * library routine: the caller passes the graph as DEVICE arrays (rowptr
+ * uint64[n+1], colidx int32[n_adj], labels uint8[n] or NULL) and gets the
+ * count in *count_out (host); the control block, root list and per-warp
+ * arenas live in one static device array of PM_STATIC_SCRATCH_BYTES.
+ *  - Limits: one plan; the root list plus one block of warp arenas
+ *    (patterns' worst-case candidate sets, sized from max_degree) must fit
+ *    the scratch, otherwise PM_ERR_INVALID says so; fewer warps run when
+ *    the arenas only partly fit.  Per-root outputs, root orders, ranges and
+ *    shards are not supported here.
+ *  - The first call on a device looks up the scratch's device address
+ *    (cudaGetSymbolAddress) with that device current; make that first call
+ *    before any stream capture.
+ *  - Every call shares the one scratch and clears what must start at zero;
+ *    calls that overlap on the GPU (other threads, other streams) race on
+ *    it -- serialize them.
+ *  - stream: a cudaStream_t (NULL = legacy default stream); the call
+ *    returns after the work on it is done.  stats_out->kernel_ms is 0. */
+pm_status pm_match_static(const uint64_t* d_rowptr, const int32_t* d_colidx, const uint8_t* d_labels,
+                          int64_t n, int64_t n_adj, int32_t max_degree, const pm_plan* plan,
+                          const pm_run_opts* opts, void* stream, uint64_t* count_out,
+                          pm_stats* stats_out);
+
 const char* pm_strerror(pm_status s);
 const char* pm_last_error(void);
 

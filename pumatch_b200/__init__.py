@@ -124,6 +124,8 @@ SIGNATURES = {
     "pm_mlp_train_step": (C.c_int, [_P, _P, _P, C.c_int64, C.c_float, C.POINTER(C.c_float)]),
     "pm_mlp_get_weights": (C.c_int, [_P, _P]),
     "pm_mlp_set_weights": (C.c_int, [_P, _P]),
+    "pm_match_static": (C.c_int, [_P, _P, _P, C.c_int64, C.c_int64, C.c_int32, _P, C.POINTER(RunOpts), _P,
+                                  C.POINTER(C.c_uint64), C.POINTER(Stats)]),
     "pm_strerror": (C.c_char_p, [C.c_int]),
     "pm_last_error": (C.c_char_p, []),
 }

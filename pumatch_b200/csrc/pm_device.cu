@@ -25,6 +25,7 @@
 #include <climits>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <vector>
 
 #include "pm_common.h"
@@ -1707,4 +1708,201 @@ extern "C" pm_status pm_query_run(pm_query* q, uint64_t* counts_out, pm_stats* s
   float kms = 0;
   CK(cudaEventElapsedTime(&kms, q->eb, q->ee));
   return finish_launch(q->L, q->h_ctl, kms, q->roots_ms, pst, counts_out, stats_out);
+}
+
+// ---------------------------------------------------------------------
+// Allocation-free entry point: pm_match_static.
+//
+// For callers that must not allocate device memory -- code running where
+// cudaMalloc is not allowed or not wanted: inside a host callback, in a
+// process whose allocator is owned by another framework with a fixed pool,
+// in a real-time service that has budgeted every byte up front, or while
+// another library holds the device allocator lock.  The caller provides the
+// graph arrays and receives the count; everything the launch needs besides
+// them (control block, donation ring, root list, per-warp arenas) lives in
+// one file-scope device array of PM_STATIC_SCRATCH_BYTES that each GPU keeps
+// from module load until the process exits.
+// ---------------------------------------------------------------------
+static __device__ __align__(256) unsigned char g_static_scratch[PM_STATIC_SCRATCH_BYTES];
+
+namespace {
+constexpr unsigned kStaticRing = 4096;  // donation slots inside the static scratch
+constexpr size_t kStaticCtlWords = 32 + 32 + 16 + 8 + kStaticRing + 6 * kStaticRing;
+
+struct StaticScratch {
+  bool ready = false;
+  unsigned char* base = nullptr;  // device address of g_static_scratch on this device
+};
+StaticScratch g_static[64];
+std::mutex g_static_mu;
+
+// Root filter with unordered, bounded compaction (no scan, no temporary
+// buffer): each warp reserves slots with one atomic per 32 edges; writes past
+// `cap` are skipped and the host sees the true total afterwards.  The 2-hop
+// test scans the neighbour's list for a vertex of sufficient degree.
+__global__ void roots_static_kernel(const uint64_t* rowptr, const int32_t* colidx, const uint8_t* labels, int64_t n,
+                                    RootFilter f, int2* out, unsigned long long cap, unsigned long long* counter) {
+  const int lane = lane_id();
+  const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
+  for (long long r = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); r < n; r += warps) {
+    const uint64_t b = rowptr[r], e = rowptr[r + 1];
+    if ((long long)(e - b) < f.d0 || (f.labeled && labels[r] != f.lab0)) continue;
+    for (uint64_t i0 = b; i0 < e; i0 += 32) {
+      const uint64_t i = i0 + lane;
+      bool keep = false;
+      int c = 0;
+      if (i < e) {
+        c = colidx[i];
+        keep = (!f.need_gt || r > c) && (!f.labeled || labels[c] == f.lab1) &&
+               (int)(rowptr[c + 1] - rowptr[c]) >= f.d1;
+        if (keep) {
+          bool two_hop = false;
+          for (uint64_t d = rowptr[c]; d < rowptr[c + 1] && !two_hop; d++) {
+            const int u = colidx[d];
+            two_hop = (int)(rowptr[u + 1] - rowptr[u]) >= f.d2;
+          }
+          keep = two_hop;
+        }
+      }
+      const unsigned bal = __ballot_sync(FULL, keep);
+      unsigned long long base = 0;
+      if (lane == 0 && bal) base = atomicAdd(counter, (unsigned long long)__popc(bal));
+      base = __shfl_sync(FULL, base, 0);
+      if (keep) {
+        const unsigned long long pos = base + __popc(bal & lanemask_lt());
+        if (pos < cap) out[pos] = make_int2((int)r, c);
+      }
+    }
+  }
+}
+}  // namespace
+
+extern "C" pm_status pm_match_static(const uint64_t* d_rowptr, const int32_t* d_colidx, const uint8_t* d_labels,
+                                     int64_t n, int64_t nadj, int32_t max_degree, const pm_plan* plan,
+                                     const pm_run_opts* opts, void* stream, uint64_t* count_out,
+                                     pm_stats* stats_out) {
+  if (!d_rowptr || (nadj > 0 && !d_colidx) || !plan || !count_out || n < 0 || max_degree < 0)
+    return fail(PM_ERR_INVALID, "pm_match_static: bad arguments");
+  const Plan& p = *plan_of(plan);
+  if (p.labeled && !d_labels) return fail(PM_ERR_INVALID, "pm_match_static: labeled plan without labels");
+  pm_run_opts o;
+  pm_run_opts_default(&o);
+  if (opts) o = *opts;
+  if (o.root_counts || o.root_cost || o.root_reads || o.root_order || o.shard_count > 1 || o.root_begin >= 0 ||
+      o.root_end >= 0)
+    return fail(PM_ERR_INVALID, "pm_match_static: per-root outputs, root orders, ranges and shards are not supported");
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return fail(PM_ERR_INVALID, "pm_match_static: device %d out of range", dev);
+  cudaStream_t st = (cudaStream_t)stream;
+  // set-up, once per device, with that device current
+  unsigned char* base = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(g_static_mu);
+    if (!g_static[dev].ready) {
+      unsigned char* ptr = nullptr;
+      cudaError_t e = cudaGetSymbolAddress((void**)&ptr, g_static_scratch);
+      if (e != cudaSuccess)
+        return fail(PM_ERR_CUDA, "pm_match_static: cudaGetSymbolAddress failed: %s", cudaGetErrorString(e));
+      g_static[dev].base = ptr;
+      g_static[dev].ready = true;
+    }
+    base = g_static[dev].base;
+  }
+  int nsm = 0;
+  CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  const int T = std::max(0, o.truncate);
+  const int wpb = o.warps_per_block > 0 ? o.warps_per_block : 8;
+  if (wpb > 16 || (wpb & (wpb - 1)))
+    return fail(PM_ERR_INVALID, "pm_match_static: warps_per_block must be 1,2,4,8 or 16");
+  const int64_t slot_words = arena_words_for(p, max_degree, T);
+  const size_t warp_bytes = (size_t)slot_words * 4;
+  const size_t ctl_bytes = kStaticCtlWords * 8;
+  const size_t min_arena = (size_t)wpb * warp_bytes;  // one block
+  if (ctl_bytes + 64 + min_arena > PM_STATIC_SCRATCH_BYTES)
+    return fail(PM_ERR_INVALID,
+                "pm_match_static: one block of warp arenas needs %zu bytes, beyond the %llu-byte static scratch "
+                "(max degree %d is too large for this entry point)",
+                min_arena, (unsigned long long)PM_STATIC_SCRATCH_BYTES, max_degree);
+  // layout: control block | root counter | roots | arenas
+  unsigned long long* ctl = (unsigned long long*)base;
+  unsigned long long* rcount = (unsigned long long*)(base + ctl_bytes);
+  int2* roots = (int2*)(base + ctl_bytes + 64);
+  const size_t after_ctl = PM_STATIC_SCRATCH_BYTES - ctl_bytes - 64;
+  const unsigned long long root_cap = (after_ctl - min_arena) / sizeof(int2);
+
+  CK(cudaMemsetAsync(base, 0, ctl_bytes + 64, st));  // previous calls leave their contents behind
+  const RootFilter f = to_filter(p);
+  (void)cudaGetLastError();  // drop a stale error from an earlier call
+  roots_static_kernel<<<4 * nsm, 256, 0, st>>>(d_rowptr, d_colidx, d_labels, n, f, roots, root_cap, rcount);
+  CK(cudaGetLastError());
+  unsigned long long nroots = 0;
+  CK(cudaMemcpyAsync(&nroots, rcount, sizeof(nroots), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  if (nroots > root_cap)
+    return fail(PM_ERR_INVALID, "pm_match_static: %llu root edges exceed the %llu the static scratch holds",
+                nroots, root_cap);
+  const size_t roots_bytes = ((size_t)nroots * sizeof(int2) + 255) & ~(size_t)255;
+  int32_t* arena = (int32_t*)((unsigned char*)roots + roots_bytes);
+  const size_t arena_bytes = after_ctl - roots_bytes;
+  int per_sm = 0;
+  auto kfn = p.labeled ? match_kernel<true, false, 1> : match_kernel<false, false, 1>;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, wpb * 32, sizeof(WarpState) * wpb));
+  int64_t blocks = std::max(1, per_sm) * (int64_t)nsm;
+  blocks = std::min<int64_t>(blocks, (int64_t)(arena_bytes / ((size_t)wpb * warp_bytes)));
+  if (blocks < 1) return fail(PM_ERR_INTERNAL, "pm_match_static: no room for a block of arenas");
+
+  DPlan dp = to_dplan(p);
+  dp.roots = roots;
+  dp.nroots = (int64_t)nroots;
+  CK(cudaMemcpyToSymbolAsync(c_plans, &dp, sizeof(DPlan), 0, cudaMemcpyHostToDevice, st));
+  MatchArgs a;
+  memset(&a, 0, sizeof(a));
+  a.rowptr = d_rowptr;
+  a.colidx = d_colidx;
+  a.labels = d_labels;
+  a.n = (int32_t)n;
+  a.nplans = 1;
+  a.T = T;
+  a.chunk = o.chunk > 0 ? o.chunk : 16;
+  a.shard_rank = 0;
+  a.shard_count = 1;
+  a.split_min = o.split_level1 == 0 ? 64 : (o.split_level1 < 0 ? 0 : o.split_level1);
+  a.maxdeg = max_degree;
+  unsigned long long* w = ctl;
+  a.cursors = w; w += 32;
+  a.counts = w; w += 32;
+  a.stats = w; w += 16;
+  a.status = (unsigned int*)w;
+  a.active = (unsigned int*)w + 1; w += 1;
+  a.don_head = w; w += 1;
+  a.don_tail = w; w += 1;
+  a.heartbeat = w; w += 5;
+  a.don_ready = w; w += kStaticRing;
+  a.don_items = (int4*)w; w += 6 * kStaticRing;
+  a.don_mask = kStaticRing - 1;
+  const int64_t warps = blocks * wpb;
+  a.total_warps = (unsigned int)warps;
+  a.arena = arena;
+  a.arena_words = slot_words;
+  a.slot_words = slot_words;
+  a.timeout_ns = (unsigned long long)(o.timeout_ms > 0 ? o.timeout_ms : 600000) * 1000000ull;
+  const unsigned int active0 = (unsigned int)warps;
+  CK(cudaMemcpyAsync(a.active, &active0, sizeof(active0), cudaMemcpyHostToDevice, st));
+  (void)cudaGetLastError();  // drop a stale error from an earlier call
+  kfn<<<(int)blocks, wpb * 32, sizeof(WarpState) * wpb, st>>>(a);
+  CK(cudaGetLastError());
+  unsigned long long host_ctl[kCtlRead];
+  CK(cudaMemcpyAsync(host_ctl, ctl, sizeof(host_ctl), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  Launch L;
+  L.nplans = 1;
+  L.plans[0] = &p;
+  L.blocks = (int)blocks;
+  L.threads = wpb * 32;
+  L.warps = warps;
+  L.a = a;
+  pm_stats pst;
+  memset(&pst, 0, sizeof(pst));
+  return finish_launch(L, host_ctl, 0.f, 0.f, pst, count_out, stats_out);
 }
