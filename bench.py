@@ -262,7 +262,7 @@ def run_ours(args, workload):
     shard = dict(shard_rank=rank, shard_count=world) if world > 1 else {}
     run_kw = dict(timeout_ms=args.timeout_s * 1000, high_occupancy=args.high_occupancy, **shard)
     if args.root_limit > 0:
-        run_kw.update(root_begin=0, root_end=args.root_limit)
+        run_kw.update(root_begin=args.root_begin, root_end=args.root_begin + args.root_limit)
 
     def one_step():
         counts, st = ctx.match(graph, plans, **run_kw)
@@ -347,9 +347,11 @@ def run_ours(args, workload):
             "data": "synthetic",
             "config": {"workload": workload, "graph": w["graph"], "labeled": w["labeled"],
                        "patterns": [p for p, _ in texts], "counts": counts_total,
-                       "kernel_variant": "high_occupancy" if args.high_occupancy else "default",
+                       "kernel_variant": ["default", "regs64", "regs85"][args.high_occupancy],
                        "root_limit": args.root_limit or None,
                        "roots": int(st["n_roots"]), "set_ops_per_step": set_ops // args.steps,
+                       "donated_ranges_last_step": int(st["splits"]),
+                       "page_misses_last_step": int(st["page_misses"]), "pages_loaded_last_step": int(st["pages_loaded"]),
                        "l2": "flushed between timed steps (256 MB write)",
                        "parallelism": f"roots sharded x{world}" if world > 1 else "1 GPU"},
             "e2e": {"value": e2e_value, "unit": "matches/s", "h2d_bytes_per_step": int(h2d),
@@ -452,8 +454,10 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--timeout-s", type=int, default=120, help="hard device-side limit per launch")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--high-occupancy", action="store_true", help="kernel variant capped at 64 registers")
-    ap.add_argument("--root-limit", type=int, default=0, help="profile a prefix of the root list only")
+    ap.add_argument("--high-occupancy", type=int, default=0,
+                    help="kernel variant: 0 no register cap, 1 capped at 64, 2 capped at 85")
+    ap.add_argument("--root-limit", type=int, default=0, help="profile this many roots only (from --root-begin)")
+    ap.add_argument("--root-begin", type=int, default=0)
     ap.add_argument("--learned", action="store_true", help="plain vs learned scheduling on the workload")
     ap.add_argument("--learn-epochs", type=int, default=20)
     args = ap.parse_args()

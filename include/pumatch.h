@@ -204,9 +204,10 @@ typedef struct {
                                the reference-ordered root list; -1 = all     */
   int64_t root_end;
   int32_t cold_cache;       /* paged mode: empty the frame pool before the run */
-  int32_t high_occupancy;   /* 1: kernel variant capped at 64 registers (more
-                               warps per SM, some spills); 0: up to 128
-                               registers, no spills (default)                */
+  int32_t high_occupancy;   /* kernel variant: 0 up to 128 registers, no
+                               spills (default); 1 capped at 64 registers
+                               (four 256-thread blocks per SM); 2 capped at
+                               85 (three blocks per SM)                      */
   int32_t reserved_[2];
   uint64_t* root_counts;    /* optional device ptr: per-root counts (plan 0) */
   float* root_cost;         /* optional device ptr: per-root set-op bytes    */

@@ -406,7 +406,7 @@ class Context:
               shard_rank: int = 0, shard_count: int = 0, root_begin: int = -1, root_end: int = -1,
               root_counts_ptr: int = 0, root_cost_ptr: int = 0, root_order_ptr: int = 0, root_reads_ptr: int = 0,
               use_graph: bool = False, timeout_ms: int = 0, cold_cache: bool = False,
-              high_occupancy: bool = False):
+              high_occupancy: int = 0):
         """Runs all patterns in one launch; returns (counts list, stats dict)."""
         o = RunOpts()
         lib().pm_run_opts_default(C.byref(o))

@@ -187,9 +187,11 @@ __device__ __forceinline__ ListRef adj(const MatchArgs& a, WarpState& S, int v, 
   return paged_list(a.pg, b, len, gather, S.pins, w.pc);
 }
 
-// The label-l part of v's list (labeled graphs in HBM), in id order.
+// The label-l part of v's list (labeled graphs in HBM), in id order; empty
+// for a label no vertex of the graph carries.
 __device__ __forceinline__ ListRef adj_label(const MatchArgs& a, int v, int l) {
   const uint64_t b = a.rowptr[v];
+  if (l >= a.nl1 - 1) return ListRef{a.colidx_lab + b, 0, -1};
   const int32_t* o = a.lab_off + (int64_t)v * a.nl1;
   const int s0 = o[l], s1 = o[l + 1];
   return ListRef{a.colidx_lab + b + s0, s1 - s0, -1};
@@ -236,6 +238,13 @@ __device__ int run_slot(const MatchArgs& a, const DPlan& P, WarpState& S, int32_
   const int32_t* B = RB.p;
   int lenA = RA.len;
   const int lenB = RB.len;
+  // a parent slot small enough goes to shared memory for the per-lane searches
+  if (kind == SLOT_INTERSECT && L > 1 && lenB <= PM_SB_MAX && !PAGED) {
+    __syncwarp();
+    for (int i = lane; i < lenB; i += 32) S.sb[i] = B[i];
+    __syncwarp();
+    B = S.sb;
+  }
 
   // symmetry-breaking upper bound (unlabeled only, src/gpu_match.cu:426-458)
   if (!LABELED && P.partial[s]) {
@@ -394,6 +403,44 @@ __device__ __forceinline__ int lane_lower_bound(const int32_t* A, int len, int x
   return lo;
 }
 
+// One lane intersects the part of sorted A[0,deg) below ub with sorted B
+// (usually in shared memory), galloping through B; four loads of A in
+// flight.  Sets *lenA to the number of elements of A below ub (the
+// reference's scan length) and returns the count of members (label-checked
+// when LABELED), or -1 when more than PM_LANE_MAX elements would be scanned
+// (the caller hands the candidate to the whole warp).
+template <bool LABELED>
+__device__ __forceinline__ int lane_intersect(const int32_t* A, int deg, int ub, const int32_t* B, int lenB,
+                                              const uint8_t* labels, uint32_t mask, int* lenA) {
+  int k = 0, p = 0, x = 0;
+  while (true) {
+    if (x >= PM_LANE_MAX) return -1;
+    int v[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) v[q] = (x + q < deg) ? A[x + q] : INT_MAX;
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const int val = v[q];
+      if (x + q >= deg || val >= ub) { *lenA = x + q; return k; }
+      int lo = p, step = 1;
+      while (lo + step < lenB && B[lo + step] < val) { lo += step; step <<= 1; }
+      int hi = min(lo + step + 1, lenB);
+      while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (B[mid] < val) lo = mid + 1; else hi = mid;
+      }
+      p = lo;
+      if (p < lenB && B[p] == val && (!LABELED || ((mask >> labels[val]) & 1u))) k++;
+      if (p >= lenB) {  // the rest of A is above all of B: only its length matters
+        const int r0 = x + q + 1;
+        *lenA = r0 + lane_lower_bound(A + r0, deg - r0, ub);
+        return k;
+      }
+    }
+    x += 4;
+  }
+}
+
 // The last level for the candidates [b, e) of level L's main slot (each is
 // v_{n-2} in turn): one lane per candidate, counting only.  Same set
 // operations and counts as run_slot(last) per candidate, organised so that
@@ -463,14 +510,28 @@ __device__ unsigned long long leaf_batch(const MatchArgs& a, const DPlan& P, War
         const uint64_t rb = a.rowptr[c];
         const int deg = (int)(a.rowptr[c + 1] - rb);
         const int32_t* A = a.colidx + rb;
+        const bool grouped = LABELED && a.colidx_lab && __popc(mask) == 1;
+        if (kind == SLOT_INTERSECT && !grouped) {
+          int lenA = 0;
+          int k = lane_intersect<LABELED>(A, deg, ub, Bs, lenB, a.labels, mask, &lenA);
+          if (k < 0) {
+            deferred = true;
+          } else {
+            if (T && k > T) k = T;
+            cnt += k;
+            bytes += 4ull * (unsigned long long)(lenA + lenB + k) + (LABELED ? (unsigned long long)lenA : 0ull);
+            ops++;
+          }
+        } else {
         const int lenA = (ub == INT_MAX) ? deg : lane_lower_bound(A, deg, ub);
-        if (LABELED && a.colidx_lab && __popc(mask) == 1) {
+        if (grouped) {
           // the label-l part of the list: a fresh set is its length, an
           // intersection merges only it
           const int32_t* o = a.lab_off + (int64_t)c * a.nl1;
           const int l = __ffs(mask) - 1;
-          const int32_t* Al = a.colidx_lab + rb + o[l];
-          const int lenl = o[l + 1] - o[l];
+          const bool present = l < a.nl1 - 1;  // a label no vertex carries: empty
+          const int32_t* Al = a.colidx_lab + rb + (present ? o[l] : 0);
+          const int lenl = present ? o[l + 1] - o[l] : 0;
           int k = 0;
           if (kind == SLOT_FRESH) {
             k = lenl;
@@ -537,6 +598,7 @@ __device__ unsigned long long leaf_batch(const MatchArgs& a, const DPlan& P, War
           cnt += k;
           bytes += 4ull * (unsigned long long)(lenA + lenB + k) + (LABELED ? (unsigned long long)lenA : 0ull);
           ops++;
+        }
         }
       }
     }
@@ -728,7 +790,8 @@ __device__ bool take_donation(const MatchArgs& a, Donation& d) {
 }
 
 // MINB = 4: 64 registers, four 256-thread blocks per SM (more warps in flight,
-// some spills); MINB = 1: up to 128 registers, no spills, fewer warps.
+// some spills); MINB = 3: 85 registers, three blocks; MINB = 1: up to 128
+// registers, no spills, fewer warps.
 template <bool LABELED, bool PAGED, int MINB>
 __global__ void __launch_bounds__(MINB == 1 ? 512 : 256, MINB) match_kernel(MatchArgs a) {
   extern __shared__ WarpState smem_state[];
@@ -1444,7 +1507,11 @@ static pm_status setup_launch(pm_ctx* c, const pm_graph* g, const pm_plan* const
   // launch geometry: persistent, occupancy-limited
   L->threads = wpb * 32;
   L->smem = sizeof(WarpState) * wpb;
-  if (!o.high_occupancy) {
+  if (o.high_occupancy == 2) {
+    if (wpb > 8) return fail(PM_ERR_INVALID, "warps_per_block 16 is not available with high_occupancy");
+    L->kfn = L->labeled ? (L->paged ? match_kernel<true, true, 3> : match_kernel<true, false, 3>)
+                        : (L->paged ? match_kernel<false, true, 3> : match_kernel<false, false, 3>);
+  } else if (!o.high_occupancy) {
     L->kfn = L->labeled ? (L->paged ? match_kernel<true, true, 1> : match_kernel<true, false, 1>)
                         : (L->paged ? match_kernel<false, true, 1> : match_kernel<false, false, 1>);
   } else {
