@@ -113,6 +113,16 @@ pm_status pm_graph_write(const char* prefix, int64_t n, int64_t n_adj,
                          const uint32_t* labels);
 void pm_host_free(void* p);
 
+/* SNAP edge list (text) -> <out_prefix>.meta.txt/.vertex.bin/.edge.bin and,
+ * when n_labels > 0, .label.bin: the reference's converter pipeline
+ * (graph_converter/convert.sh:32-65: snapToBin, makeLists, compactify,
+ * labelize) in one pass.  Ids are compacted in first-seen order; lists are
+ * symmetrised, sorted and deduplicated; self-loops are dropped unless
+ * keep_self_loops; labels are std::rand() % n_labels after std::srand(0)
+ * (labelize.cpp uses 10). */
+pm_status pm_convert_snap(const char* snap_path, const char* out_prefix, int n_labels,
+                          int keep_self_loops, int64_t* n_vertices, int64_t* n_adj);
+
 /* ------------------------------------------------------------------ */
 /* Synthetic inputs (stand-ins for the reference's converted datasets)  */
 /* ------------------------------------------------------------------ */

@@ -96,6 +96,8 @@ SIGNATURES = {
                                 C.POINTER(C.c_int32), _PP, _PP, _PP]),
     "pm_graph_write": (C.c_int, [C.c_char_p, C.c_int64, C.c_int64, _P, _P, _P]),
     "pm_host_free": (None, [_P]),
+    "pm_convert_snap": (C.c_int, [C.c_char_p, C.c_char_p, C.c_int, C.c_int, C.POINTER(C.c_int64),
+                                  C.POINTER(C.c_int64)]),
     "pm_gen_chung_lu": (C.c_int, [C.c_int64, C.c_int64, C.c_double, C.c_double, C.c_double, C.c_uint64,
                                   _PP, _PP, C.POINTER(C.c_int64), C.POINTER(C.c_int32)]),
     "pm_gen_rmat": (C.c_int, [C.c_int64, C.c_int64, C.c_double, C.c_double, C.c_double, C.c_uint64,
@@ -207,6 +209,16 @@ class HostGraph:
         colidx = _take(ci, nadj.value, np.int32)
         labels = _take(lb, n.value, np.uint32) if labeled else None
         return HostGraph(rowptr, colidx, labels)
+
+
+def convert_snap(snap_path: str, out_prefix: Optional[str] = None, n_labels: int = 10,
+                 keep_self_loops: bool = False):
+    """SNAP text -> the reference's CSR files (default prefix: the text path,
+    as graph_converter/convert.sh names them).  Returns (n_vertices, n_adj)."""
+    n, nadj = C.c_int64(), C.c_int64()
+    _check(lib().pm_convert_snap(snap_path.encode(), (out_prefix or snap_path).encode(), n_labels,
+                                 int(keep_self_loops), C.byref(n), C.byref(nadj)))
+    return n.value, nadj.value
 
 
 def gen_chung_lu(n: int, n_edges: int, gamma: float = 2.1, i0: float = 10.0, max_w: float = 5000.0,
@@ -472,5 +484,5 @@ def match(g: GraphPreprocessor, patterns, ctx: Optional[Context] = None, **kw):
 
 __all__ = [
     "PmError", "HostGraph", "GraphPreprocessor", "PatternPreprocessor", "Context", "Query", "match",
-    "gen_chung_lu", "gen_rmat", "gen_labels", "lib", "LIB_PATH", "CLI_PATH", "SIGNATURES",
+    "gen_chung_lu", "gen_rmat", "gen_labels", "convert_snap", "lib", "LIB_PATH", "CLI_PATH", "SIGNATURES",
 ]

@@ -19,6 +19,7 @@ INC = os.path.join(ROOT, "include")
 BUILD = os.path.join(PKG, "_build")
 LIB = os.path.join(PKG, "lib", "libpumatch_b200.so")
 CLI = os.path.join(PKG, "bin", "test")
+CONVERT = os.path.join(PKG, "bin", "convert")
 CUDA = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA, "bin", "nvcc")
 
@@ -77,6 +78,10 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> str:
         _run(["g++", "-O2", "-std=c++17", "-I", INC, "-o", CLI, cli_src,
               "-L", os.path.dirname(LIB), "-lpumatch_b200",
               "-Wl,-rpath,$ORIGIN/../lib"])
+    conv_src = os.path.join(CSRC, "pm_convert_cli.cpp")
+    if _stale(CONVERT, [conv_src, LIB, os.path.join(INC, "pumatch.h")]):
+        _run(["g++", "-O2", "-std=c++17", "-I", INC, "-o", CONVERT, conv_src,
+              "-L", os.path.dirname(LIB), "-lpumatch_b200", "-Wl,-rpath,$ORIGIN/../lib"])
     return LIB
 
 

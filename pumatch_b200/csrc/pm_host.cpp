@@ -7,6 +7,7 @@
 #include <omp.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <atomic>
 #include <cmath>
 #include <cstdarg>
@@ -587,5 +588,97 @@ extern "C" pm_status pm_gen_labels(int64_t n, int n_labels, uint64_t seed, uint3
     for (int64_t v = b * kBlock; v < e; v++) lab[v] = r.below((uint32_t)n_labels);
   }
   *labels = lab;
+  return PM_OK;
+}
+
+// ---------------------------------------------------------------- converter
+
+// SNAP edge list -> the CSR files (graph_converter/convert.sh:32-65 as one
+// step): '#' and empty lines skipped, the first two integers of a line are an
+// edge; ids are compacted in first-seen order (snapToBin.cpp:23-32), every
+// edge is stored in both directions, each list sorted and deduplicated
+// (compactify.cpp:15-21).  Self-loops are dropped unless keep_self_loops (the
+// reference keeps them; the matcher assumes none).  n_labels > 0 writes
+// labels std::rand() % n_labels after std::srand(0), vertex by vertex, which
+// is labelize.cpp:45-49's sequence with n_labels = 10.
+extern "C" pm_status pm_convert_snap(const char* snap_path, const char* out_prefix, int n_labels,
+                                     int keep_self_loops, int64_t* n_out, int64_t* nadj_out) {
+  if (!snap_path || !out_prefix || n_labels < 0 || n_labels > 32)
+    return fail(PM_ERR_INVALID, "pm_convert_snap: bad arguments");
+  std::ifstream in(snap_path);
+  if (!in.good()) return fail(PM_ERR_IO, "cannot open %s", snap_path);
+  std::vector<int64_t> id_map;
+  int64_t next_id = 0;
+  auto map_id = [&](int64_t raw) -> int64_t {
+    if (raw < 0) return -1;
+    if ((int64_t)id_map.size() <= raw) id_map.resize((size_t)raw + 2048, -1);
+    if (id_map[raw] < 0) id_map[raw] = next_id++;
+    return id_map[raw];
+  };
+  std::vector<uint64_t> keys;
+  std::vector<uint32_t> loops;
+  std::string line;
+  int64_t lineno = 0;
+  while (std::getline(in, line)) {
+    lineno++;
+    if (line.empty() || line[0] == '#') continue;
+    std::istringstream ls(line);
+    long long a = -1, b = -1;
+    if (!(ls >> a >> b)) return fail(PM_ERR_FORMAT, "%s line %lld: expected two vertex ids", snap_path, (long long)lineno);
+    const int64_t u = map_id(a), v = map_id(b);
+    if (u < 0 || v < 0) return fail(PM_ERR_FORMAT, "%s line %lld: negative vertex id", snap_path, (long long)lineno);
+    if (u > INT32_MAX - 1 || v > INT32_MAX - 1) return fail(PM_ERR_FORMAT, "%s: more than 2^31 vertices", snap_path);
+    if (u == v) {
+      if (keep_self_loops) loops.push_back((uint32_t)u);
+      continue;
+    }
+    keys.push_back(edge_key((uint32_t)u, (uint32_t)v));
+  }
+  const int64_t n = next_id;
+  __gnu_parallel::sort(keys.begin(), keys.end());
+  keys.erase(std::unique(keys.begin(), keys.end()), keys.end());
+  uint64_t* rowptr = nullptr;
+  int32_t* colidx = nullptr;
+  int64_t nadj = 0;
+  int32_t maxd = 0;
+  csr_from_keys(n, keys, &rowptr, &colidx, &nadj, &maxd);
+  if (!loops.empty()) {
+    // add u to its own list once, keeping lists sorted
+    std::sort(loops.begin(), loops.end());
+    loops.erase(std::unique(loops.begin(), loops.end()), loops.end());
+    uint64_t* rp2 = (uint64_t*)malloc(sizeof(uint64_t) * (n + 1));
+    int32_t* ci2 = (int32_t*)malloc(sizeof(int32_t) * (size_t)(nadj + (int64_t)loops.size() + 1));
+    size_t li = 0;
+    rp2[0] = 0;
+    for (int64_t v = 0; v < n; v++) {
+      const bool self = li < loops.size() && loops[li] == (uint32_t)v;
+      int64_t o = (int64_t)rp2[v];
+      bool placed = !self;
+      for (uint64_t e = rowptr[v]; e < rowptr[v + 1]; e++) {
+        if (!placed && colidx[e] > v) { ci2[o++] = (int32_t)v; placed = true; }
+        ci2[o++] = colidx[e];
+      }
+      if (!placed) ci2[o++] = (int32_t)v;
+      if (self) li++;
+      rp2[v + 1] = (uint64_t)o;
+    }
+    free(rowptr);
+    free(colidx);
+    rowptr = rp2;
+    colidx = ci2;
+    nadj = (int64_t)rp2[n];
+  }
+  std::vector<uint32_t> labels;
+  if (n_labels > 0) {
+    labels.resize((size_t)std::max<int64_t>(n, 1));
+    std::srand(0);
+    for (int64_t v = 0; v < n; v++) labels[v] = (uint32_t)(std::rand() % n_labels);
+  }
+  pm_status st = pm_graph_write(out_prefix, n, nadj, rowptr, colidx, n_labels > 0 ? labels.data() : nullptr);
+  free(rowptr);
+  free(colidx);
+  if (st != PM_OK) return st;
+  if (n_out) *n_out = n;
+  if (nadj_out) *nadj_out = nadj;
   return PM_OK;
 }
