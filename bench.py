@@ -47,23 +47,24 @@ WORKLOADS = {
     # the same graph with 16 uniform labels and the 7-cycle (labeled semantics)
     "chunglu100k_c7_lab16": dict(graph=_CL100K, labeled=True, n_labels=16, label_seed=102, pattern_label_seed=202,
                                  patterns=[("C7", P.cycle(7))]),
-    # the K7 query with the adjacency in host memory and a frame pool of 1/8
-    # of it (the reference's out-of-core mode on the C1 graph)
+    # the K7 query with the adjacency in host memory: half of it in static
+    # frames (the reference's device partition holds the first 60% of the
+    # edges) plus an evictable tenth
     "chunglu100k_k7_paged": dict(graph=_CL100K, labeled=False, n_labels=0, patterns=[("K7", P.clique(7))],
-                                 paged=dict(frame_fraction=0.125, page_bytes=16 << 10)),
+                                 paged=dict(frame_fraction=0.6, static_fraction=0.5, page_bytes=16 << 10)),
     # R-MAT (a,b,c = .57,.19,.19) 1M vertices / 16M edges, 32 labels, the
-    # 5-cycle plus 2-vertex pendant path, in HBM and paged (pool = 1/4)
+    # 5-cycle plus 2-vertex pendant path, in HBM and paged (the same pool split)
     "rmat1m_c5t2_lab32": dict(graph=_RMAT1M, labeled=True, n_labels=32, label_seed=102, pattern_label_seed=202,
                               patterns=[("C5t2", P.cycle_tail(5, 2))]),
     "rmat1m_c5t2_lab32_paged": dict(graph=_RMAT1M, labeled=True, n_labels=32, label_seed=102,
                                     pattern_label_seed=202, patterns=[("C5t2", P.cycle_tail(5, 2))],
-                                    paged=dict(frame_fraction=0.25, page_bytes=64 << 10)),
+                                    paged=dict(frame_fraction=0.6, static_fraction=0.5, page_bytes=64 << 10)),
     # twenty seeded 4-7-vertex patterns in one persistent launch
     "rmat128k_batch20_lab32": dict(graph=_RMAT128K, labeled=True, n_labels=32, label_seed=102, batch_seed=303),
     # learned-scheduler comparison (--learned): trained on seeds 11, 12, 13
     "rmat128k_c5t2_lab32_paged": dict(graph=_RMAT128K, labeled=True, n_labels=32, label_seed=102,
                                       pattern_label_seed=202, patterns=[("C5t2", P.cycle_tail(5, 2))],
-                                      paged=dict(frame_fraction=0.25, page_bytes=16 << 10)),
+                                      paged=dict(frame_fraction=0.3, static_fraction=0.25, page_bytes=16 << 10)),
 }
 DEFAULT_WORKLOAD = "chunglu100k_k7"
 
@@ -95,9 +96,11 @@ def place_graph(w, hg, device):
     pg = w.get("paged")
     if not pg:
         return pm.GraphPreprocessor.from_host(hg, labeled=w["labeled"], device=device)
-    pool = max(pg["page_bytes"], int(hg.colidx.nbytes * pg["frame_fraction"]) // pg["page_bytes"] * pg["page_bytes"])
+    pb = pg["page_bytes"]
+    pool = max(pb, int(hg.colidx.nbytes * pg["frame_fraction"]) // pb * pb)
+    static = int(hg.colidx.nbytes * pg.get("static_fraction", 0.0)) // pb * pb
     return pm.GraphPreprocessor.from_host(hg, labeled=w["labeled"], device=device, paged=True,
-                                          page_bytes=pg["page_bytes"], frame_pool_bytes=pool)
+                                          page_bytes=pb, frame_pool_bytes=pool, static_pool_bytes=static)
 
 
 def dist_env():
@@ -445,6 +448,52 @@ def run_learned(args, workload):
     print(json.dumps(line), flush=True)
 
 
+def run_batch_compare(args, workload):
+    """One batched persistent launch (and its CUDA-graph replay) vs the same
+    patterns launched one by one; optional autotuner sweep."""
+    import torch
+    torch.cuda.set_device(0)
+    ctx = pm.Context(0)
+    w, hg, texts = build_workload(workload)
+    labeled = w["labeled"]
+    g = place_graph(w, hg, 0)
+    plans = [pm.PatternPreprocessor(text=t, labeled=labeled) for _, t in texts]
+    kw = dict(timeout_ms=args.timeout_s * 1000)
+    for _ in range(args.warmup):
+        ctx.match(g, plans, **kw)
+    batched = []
+    for _ in range(args.steps):
+        c, st = ctx.match(g, plans, **kw)
+        batched.append(st["kernel_ms"] + st["roots_ms"])
+    q = ctx.prepare(g, plans, **kw)
+    replay = []
+    for _ in range(args.steps):
+        cq, sq = q.run()
+        assert cq == c
+        replay.append(sq["kernel_ms"])
+    seq = []
+    for _ in range(args.steps):
+        tot, cs = 0.0, []
+        for p in plans:
+            c1, s1 = ctx.match(g, [p], **kw)
+            tot += s1["kernel_ms"] + s1["roots_ms"]
+            cs.append(c1[0])
+        assert cs == c
+        seq.append(tot)
+    line = {"metric": "batched_vs_sequential_ms", "workload": workload, "patterns": [n for n, _ in texts],
+            "counts": c, "batched_ms": statistics.median(batched), "graph_replay_kernel_ms": statistics.median(replay),
+            "sequential_ms": statistics.median(seq),
+            "speedup": statistics.median(seq) / statistics.median(batched)}
+    if args.autotune:
+        from pumatch_b200 import autotune
+        rows = autotune.sweep(ctx, g, plans, warps=(4, 8, 16), chunks=(32, 256, 2048), splits=(16, 64),
+                              timeout_ms=args.timeout_s * 1000)
+        best = min(rows, key=lambda r: r["kernel_ms"])
+        line["autotune"] = {"best": best, "default_kernel_ms": statistics.median(batched), "configs": len(rows),
+                            "results": rows}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -460,9 +509,13 @@ def main():
     ap.add_argument("--root-begin", type=int, default=0)
     ap.add_argument("--learned", action="store_true", help="plain vs learned scheduling on the workload")
     ap.add_argument("--learn-epochs", type=int, default=20)
+    ap.add_argument("--compare-sequential", action="store_true", help="batched vs one launch per pattern")
+    ap.add_argument("--autotune", action="store_true", help="with --compare-sequential: sweep launch configs")
     args = ap.parse_args()
     if args.learned:
         run_learned(args, args.workload)
+    elif args.compare_sequential:
+        run_batch_compare(args, args.workload)
     elif args.impl == "reference":
         run_reference(args, args.workload)
     else:

@@ -56,6 +56,9 @@ typedef struct {
   int residency;            /* PM_RESIDENT_*                                   */
   uint32_t page_bytes;      /* paged mode: page size (multiple of 4 KiB)       */
   uint64_t frame_pool_bytes;/* paged mode: device frame-pool cap               */
+  uint64_t static_pool_bytes;/* paged mode: the part of the pool whose pages are
+                               placed once and never evicted (the reference's
+                               device partition, test.cu:22-43); 0 = none     */
 } pm_graph_opts;
 
 typedef struct {
@@ -68,6 +71,7 @@ typedef struct {
   uint64_t device_bytes;    /* device memory held by the graph                 */
   uint64_t n_pages;         /* paged mode: pages of the adjacency array        */
   uint64_t n_frames;        /* paged mode: frames in the device pool           */
+  uint64_t n_static_frames; /* paged mode: frames never evicted               */
 } pm_graph_info;
 
 void pm_graph_opts_default(pm_graph_opts* o);
@@ -95,7 +99,9 @@ pm_status pm_graph_get_info(const pm_graph* g, pm_graph_info* info);
 
 /* Paged graphs: the pages (indices of page_bytes-sized ranges of the adjacency
  * array) the frame pool holds at the start of every run that is not cold --
- * by default the first n_frames pages.  Replaces the reference's initial
+ * by default the first n_frames pages.  The first n_static_frames of the list
+ * fill the static frames (in ascending page order) and stay there in cold runs
+ * too; the rest fill the evictable frames.  Replaces the reference's initial
  * package build over the vertices past the device partition
  * (src/buffer.cu:986-1060 create_buffer_from_graph). */
 pm_status pm_graph_set_resident_pages(pm_graph* g, const int64_t* pages, int64_t n);
@@ -234,7 +240,7 @@ typedef struct {
   uint64_t set_ops;         /* executed set operations                      */
   uint64_t alg_bytes;       /* sum over set ops of 4(|A|+|B|+|C|) (+|A|
                                label bytes when labeled) + 8 per root       */
-  uint64_t splits;          /* level-1 ranges donated between warps         */
+  uint64_t splits;          /* ranges donated between warps (any level)     */
   uint64_t page_hits;       /* paged mode: adjacency reads served from HBM  */
   uint64_t page_misses;     /* paged mode: reads served over the host link  */
   uint64_t h2d_page_bytes;  /* paged mode: bytes copied into frames         */
@@ -248,6 +254,9 @@ typedef struct {
   uint64_t arena_bytes;
   uint32_t device_status;   /* 0 ok; else PM_DEV_* flags                     */
   uint32_t pad_;
+  uint64_t warp_ns;         /* sum over warps of their time in the launch    */
+  uint64_t idle_ns;         /* sum over warps of time spent waiting for
+                               donated work once the root queue was empty   */
 } pm_stats;
 
 /* Replaces the `_parallel_match` launch and the host reduction of per-warp

@@ -40,13 +40,14 @@ class PmError(RuntimeError):
 
 class GraphOpts(C.Structure):
     _fields_ = [("labeled", C.c_int), ("device", C.c_int), ("residency", C.c_int),
-                ("page_bytes", C.c_uint32), ("frame_pool_bytes", C.c_uint64)]
+                ("page_bytes", C.c_uint32), ("frame_pool_bytes", C.c_uint64), ("static_pool_bytes", C.c_uint64)]
 
 
 class GraphInfo(C.Structure):
     _fields_ = [("n_vertices", C.c_int64), ("n_adj", C.c_int64), ("max_degree", C.c_int32),
                 ("labeled", C.c_int32), ("n_labels", C.c_int32), ("residency", C.c_int32),
-                ("device_bytes", C.c_uint64), ("n_pages", C.c_uint64), ("n_frames", C.c_uint64)]
+                ("device_bytes", C.c_uint64), ("n_pages", C.c_uint64), ("n_frames", C.c_uint64),
+                ("n_static_frames", C.c_uint64)]
 
 
 class PlanDesc(C.Structure):
@@ -73,7 +74,8 @@ class Stats(C.Structure):
                 ("h2d_page_bytes", C.c_uint64), ("zero_copy_bytes", C.c_uint64),
                 ("pages_loaded", C.c_uint64), ("evictions", C.c_uint64), ("kernel_ms", C.c_float),
                 ("roots_ms", C.c_float), ("grid_blocks", C.c_int32), ("block_threads", C.c_int32),
-                ("arena_bytes", C.c_uint64), ("device_status", C.c_uint32), ("pad_", C.c_uint32)]
+                ("arena_bytes", C.c_uint64), ("device_status", C.c_uint32), ("pad_", C.c_uint32),
+                ("warp_ns", C.c_uint64), ("idle_ns", C.c_uint64)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_ if not k.endswith("_")}
@@ -300,18 +302,19 @@ class GraphPreprocessor:
 
     def __init__(self, prefix: Optional[str] = None, *, labeled: bool = True, device: int = 0,
                  paged: bool = False, frame_pool_bytes: int = 4 << 30, page_bytes: int = 64 << 10,
+                 static_pool_bytes: int = 0,
                  _handle=None):
         self._h = None
         if _handle is not None:
             self._h = _handle
             return
-        o = self._opts(labeled, device, paged, frame_pool_bytes, page_bytes)
+        o = self._opts(labeled, device, paged, frame_pool_bytes, page_bytes, static_pool_bytes)
         h = C.c_void_p()
         _check(lib().pm_graph_open(prefix.encode(), C.byref(o), C.byref(h)))
         self._h = h
 
     @staticmethod
-    def _opts(labeled, device, paged, frame_pool_bytes, page_bytes) -> GraphOpts:
+    def _opts(labeled, device, paged, frame_pool_bytes, page_bytes, static_pool_bytes=0) -> GraphOpts:
         o = GraphOpts()
         lib().pm_graph_opts_default(C.byref(o))
         o.labeled = int(labeled)
@@ -319,12 +322,14 @@ class GraphPreprocessor:
         o.residency = PM_RESIDENT_PAGED if paged else PM_RESIDENT_HBM
         o.frame_pool_bytes = frame_pool_bytes
         o.page_bytes = page_bytes
+        o.static_pool_bytes = static_pool_bytes
         return o
 
     @classmethod
     def from_host(cls, hg: HostGraph, *, labeled: bool = False, device: int = 0, paged: bool = False,
-                  frame_pool_bytes: int = 4 << 30, page_bytes: int = 64 << 10) -> "GraphPreprocessor":
-        o = cls._opts(labeled, device, paged, frame_pool_bytes, page_bytes)
+                  frame_pool_bytes: int = 4 << 30, page_bytes: int = 64 << 10,
+                  static_pool_bytes: int = 0) -> "GraphPreprocessor":
+        o = cls._opts(labeled, device, paged, frame_pool_bytes, page_bytes, static_pool_bytes)
         h = C.c_void_p()
         _check(lib().pm_graph_from_host(hg.n, hg.n_adj, _ptr(hg.rowptr), _ptr(hg.colidx),
                                         _ptr(hg.labels) if labeled else None, C.byref(o), C.byref(h)))

@@ -1,7 +1,7 @@
 // pm_cli.cpp -- the drop-in `test` command.
 //
 //   test <graph-prefix> <pattern.g> [--labeled=0|1] [--truncate=N] [--device=D]
-//        [--paged] [--frame-mb=M] [--page-kb=K] [--batch=<list file>]
+//        [--paged] [--frame-mb=M] [--static-mb=S] [--page-kb=K] [--batch=<list file>]
 //
 // Same positional arguments and output as the reference's driver
 // (test.cu:15-21, 200-209): the last stdout line is "<kernel ms> <count>" and
@@ -30,13 +30,13 @@ static int die(const char* what, pm_status s) {
 int main(int argc, char** argv) {
   if (argc < 3) {
     fprintf(stderr, "usage: test <graph-prefix> <pattern.g> [--labeled=0|1] [--truncate=N] [--device=D]\n"
-                    "            [--paged] [--frame-mb=M] [--page-kb=K] [--batch=<list>]\n");
+                    "            [--paged] [--frame-mb=M] [--static-mb=S] [--page-kb=K] [--batch=<list>]\n");
     return 2;
   }
   const char* prefix = argv[1];
   std::string pattern = argv[2];
   int labeled = 1, truncate = 0, device = 0, paged = 0;
-  long long frame_mb = 4096, page_kb = 64;
+  long long frame_mb = 4096, static_mb = 0, page_kb = 64;
   std::string batch;
   for (int i = 3; i < argc; i++) {
     const char* a = argv[i];
@@ -45,6 +45,7 @@ int main(int argc, char** argv) {
     else if (!strncmp(a, "--device=", 9)) device = atoi(a + 9);
     else if (!strcmp(a, "--paged")) paged = 1;
     else if (!strncmp(a, "--frame-mb=", 11)) frame_mb = atoll(a + 11);
+    else if (!strncmp(a, "--static-mb=", 12)) static_mb = atoll(a + 12);
     else if (!strncmp(a, "--page-kb=", 10)) page_kb = atoll(a + 10);
     else if (!strncmp(a, "--batch=", 8)) batch = a + 8;
     else { fprintf(stderr, "test: unknown option %s\n", a); return 2; }
@@ -68,6 +69,7 @@ int main(int argc, char** argv) {
     go.residency = PM_RESIDENT_PAGED;
     go.frame_pool_bytes = (uint64_t)frame_mb << 20;
     go.page_bytes = (uint32_t)(page_kb << 10);
+    go.static_pool_bytes = (uint64_t)static_mb << 20;
   }
   pm_graph* g = nullptr;
   pm_status s = pm_graph_open(prefix, &go, &g);

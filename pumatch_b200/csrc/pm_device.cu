@@ -111,7 +111,7 @@ struct MatchArgs {
 };
 
 enum { ST_SETOPS = 0, ST_BYTES = 1, ST_ROOTS = 2, ST_SPLITS = 3, ST_HITS = 4, ST_MISSES = 5,
-       ST_ZC_BYTES = 6, ST_REQUESTS = 7, ST_EVICTIONS = 8, ST_DROPPED = 9 };
+       ST_ZC_BYTES = 6, ST_REQUESTS = 7, ST_EVICTIONS = 8, ST_DROPPED = 9, ST_WARP_NS = 10, ST_IDLE_NS = 11 };
 
 #define PM_SB_MAX 512      // ints of a leaf batch's common operand kept in shared memory
 #define PM_LANE_MAX 96     // longest first operand one lane handles alone in a leaf batch
@@ -394,11 +394,12 @@ __device__ __forceinline__ int run_level(const MatchArgs& a, const DPlan& P, War
 }
 
 // First index of sorted A[0,len) whose element is >= x (one lane).
+template <bool CG = false>
 __device__ __forceinline__ int lane_lower_bound(const int32_t* A, int len, int x) {
   int lo = 0, hi = len;
   while (lo < hi) {
     const int mid = (lo + hi) >> 1;
-    if (A[mid] < x) lo = mid + 1; else hi = mid;
+    if (ld<CG>(A + mid) < x) lo = mid + 1; else hi = mid;
   }
   return lo;
 }
@@ -409,7 +410,7 @@ __device__ __forceinline__ int lane_lower_bound(const int32_t* A, int len, int x
 // reference's scan length) and returns the count of members (label-checked
 // when LABELED), or -1 when more than PM_LANE_MAX elements would be scanned
 // (the caller hands the candidate to the whole warp).
-template <bool LABELED>
+template <bool LABELED, bool CG>
 __device__ __forceinline__ int lane_intersect(const int32_t* A, int deg, int ub, const int32_t* B, int lenB,
                                               const uint8_t* labels, uint32_t mask, int* lenA) {
   int k = 0, p = 0, x = 0;
@@ -417,7 +418,7 @@ __device__ __forceinline__ int lane_intersect(const int32_t* A, int deg, int ub,
     if (x >= PM_LANE_MAX) return -1;
     int v[4];
 #pragma unroll
-    for (int q = 0; q < 4; q++) v[q] = (x + q < deg) ? A[x + q] : INT_MAX;
+    for (int q = 0; q < 4; q++) v[q] = (x + q < deg) ? ld<CG>(A + x + q) : INT_MAX;
 #pragma unroll
     for (int q = 0; q < 4; q++) {
       const int val = v[q];
@@ -433,7 +434,7 @@ __device__ __forceinline__ int lane_intersect(const int32_t* A, int deg, int ub,
       if (p < lenB && B[p] == val && (!LABELED || ((mask >> labels[val]) & 1u))) k++;
       if (p >= lenB) {  // the rest of A is above all of B: only its length matters
         const int r0 = x + q + 1;
-        *lenA = r0 + lane_lower_bound(A + r0, deg - r0, ub);
+        *lenA = r0 + lane_lower_bound<CG>(A + r0, deg - r0, ub);
         return k;
       }
     }
@@ -452,7 +453,7 @@ __device__ __forceinline__ int lane_intersect(const int32_t* A, int deg, int ub,
 //   * a labeled copy is the same for every candidate: counted once;
 //   * candidates whose first operand is longer than PM_LANE_MAX go back to the
 //     warp-cooperative run_slot.
-template <bool LABELED>
+template <bool LABELED, bool PAGED>
 __device__ unsigned long long leaf_batch(const MatchArgs& a, const DPlan& P, WarpState& S, int32_t* arena, int L,
                                          int b, int e, Work& w) {
   const int lane = lane_id();
@@ -491,6 +492,7 @@ __device__ unsigned long long leaf_batch(const MatchArgs& a, const DPlan& P, War
     Bs = S.sb;
   }
   unsigned long long cnt = 0, bytes = 0, ops = 0;  // per lane
+  unsigned long long lpc_hits = 0;                 // per lane (paged residency)
   for (int base = b; base < e; base += 32) {
     const int i = base + lane;
     const bool mine = i < e;
@@ -509,11 +511,34 @@ __device__ unsigned long long leaf_batch(const MatchArgs& a, const DPlan& P, War
       } else {
         const uint64_t rb = a.rowptr[c];
         const int deg = (int)(a.rowptr[c + 1] - rb);
-        const int32_t* A = a.colidx + rb;
-        const bool grouped = LABELED && a.colidx_lab && __popc(mask) == 1;
-        if (kind == SLOT_INTERSECT && !grouped) {
+        const int32_t* A = PAGED ? nullptr : a.colidx + rb;
+        int32_t pinned = -1;
+        if (PAGED) {
+          // this lane's own list when its one page is resident (pinned and
+          // read from the frame); a missing page or a list over several pages
+          // goes to the warp, which reads host memory coalesced, gathers and
+          // requests the page
+          const int sh = a.pg.page_shift;
+          const int32_t p0 = (int32_t)(rb >> sh);
+          const int32_t p1 = deg ? (int32_t)((rb + (uint64_t)deg - 1) >> sh) : p0;
+          if (deg == 0) {
+            A = a.pg.host_colidx + rb;  // nothing is read
+          } else {
+            const int32_t f = (p0 == p1) ? (pinned = try_pin(a.pg, p0)) : static_run(a.pg, p0, p1);
+            if (f < 0) {
+              deferred = true;
+            } else {
+              A = a.pg.frames + ((uint64_t)f << sh) + (rb & ((1ull << sh) - 1));
+              lpc_hits++;
+            }
+          }
+        }
+        const bool grouped = LABELED && !PAGED && a.colidx_lab && __popc(mask) == 1;
+        if (deferred) {
+          // handled by the warp below
+        } else if (kind == SLOT_INTERSECT && !grouped) {
           int lenA = 0;
-          int k = lane_intersect<LABELED>(A, deg, ub, Bs, lenB, a.labels, mask, &lenA);
+          int k = lane_intersect<LABELED, PAGED>(A, deg, ub, Bs, lenB, a.labels, mask, &lenA);
           if (k < 0) {
             deferred = true;
           } else {
@@ -523,7 +548,7 @@ __device__ unsigned long long leaf_batch(const MatchArgs& a, const DPlan& P, War
             ops++;
           }
         } else {
-        const int lenA = (ub == INT_MAX) ? deg : lane_lower_bound(A, deg, ub);
+        const int lenA = (ub == INT_MAX) ? deg : lane_lower_bound<PAGED>(A, deg, ub);
         if (grouped) {
           // the label-l part of the list: a fresh set is its length, an
           // intersection merges only it
@@ -565,8 +590,8 @@ __device__ unsigned long long leaf_batch(const MatchArgs& a, const DPlan& P, War
           int k = lim;
           for (int j = 0; j <= L; j++) {
             const int pj = S.path[j];
-            const int pos = lane_lower_bound(A, lim, pj);
-            k -= (pos < lim && A[pos] == pj) ? 1 : 0;
+            const int pos = lane_lower_bound<PAGED>(A, lim, pj);
+            k -= (pos < lim && ld<PAGED>(A + pos) == pj) ? 1 : 0;
           }
           cnt += k;
           bytes += 4ull * (unsigned long long)(lenA + k);
@@ -575,7 +600,7 @@ __device__ unsigned long long leaf_batch(const MatchArgs& a, const DPlan& P, War
           deferred = true;
         } else if (kind == SLOT_FRESH) {  // labeled: label filter only
           int k = 0;
-          for (int x = 0; x < lenA; x++) k += (mask >> a.labels[A[x]]) & 1u;
+          for (int x = 0; x < lenA; x++) k += (mask >> a.labels[ld<PAGED>(A + x)]) & 1u;
           if (T && k > T) k = T;
           cnt += k;
           bytes += 4ull * (unsigned long long)(lenA + k) + (unsigned long long)lenA;
@@ -583,7 +608,7 @@ __device__ unsigned long long leaf_batch(const MatchArgs& a, const DPlan& P, War
         } else {  // intersection with the common operand
           int k = 0, p = 0;
           for (int x = 0; x < lenA && p < lenB; x++) {
-            const int v = A[x];
+            const int v = ld<PAGED>(A + x);
             int lo = p, step = 1;
             while (lo + step < lenB && Bs[lo + step] < v) { lo += step; step <<= 1; }
             int hi = min(lo + step + 1, lenB);
@@ -600,6 +625,7 @@ __device__ unsigned long long leaf_batch(const MatchArgs& a, const DPlan& P, War
           ops++;
         }
         }
+        if (PAGED && pinned >= 0) unpin_frame(a.pg, pinned);
       }
     }
     // long first operands: the warp takes them one by one
@@ -610,8 +636,12 @@ __device__ unsigned long long leaf_batch(const MatchArgs& a, const DPlan& P, War
       const int cc = __shfl_sync(FULL, c, src);
       if (lane == 0) S.path[Lf] = cc;
       __syncwarp();
-      cnt_warp += (unsigned long long)run_slot<LABELED, false>(a, P, S, arena, Lf, s, S.top[Lf], true, w);
+      cnt_warp += (unsigned long long)run_slot<LABELED, PAGED>(a, P, S, arena, Lf, s, S.top[Lf], true, w);
     }
+  }
+  if (PAGED) {
+    for (int o = 16; o; o >>= 1) lpc_hits += __shfl_xor_sync(FULL, lpc_hits, o);
+    w.pc.hits += lpc_hits;
   }
   for (int o = 16; o; o >>= 1) {
     cnt += __shfl_xor_sync(FULL, cnt, o);
@@ -712,9 +742,9 @@ __device__ unsigned long long dfs_from(const MatchArgs& a, const DPlan& P, WarpS
     const int m = P.level_begin[L];
     const int it = S.iter[L];
     const int iend = S.iend[L];
-    if (!PAGED && it < iend && L + 1 == n - 2) {
+    if (it < iend && L + 1 == n - 2) {
       const int e2 = min(iend, it + PM_LEAF_BATCH);
-      cnt += leaf_batch<LABELED>(a, P, S, arena, L, it, e2, w);
+      cnt += leaf_batch<LABELED, PAGED>(a, P, S, arena, L, it, e2, w);
       if (lane == 0) S.iter[L] = e2;
       __syncwarp();
       if (w.err) return 0;
@@ -848,9 +878,12 @@ __global__ void __launch_bounds__(MINB == 1 ? 512 : 256, MINB) match_kernel(Matc
   if (lane == 0) atomicSub(a.active, 1u);
   __syncwarp();
   unsigned long long last_beat = 0, last_change = global_ns();
+  const unsigned long long t_drain = last_change;
+  unsigned long long busy_ns = 0;
   while (!w.err) {
     Donation item;
     if (take_donation(a, item)) {
+      const unsigned long long t_item = global_ns();
       const DPlan& P = c_plans[item.plan];
       const int2 e = P.roots[item.root];
       if (lane == 0) {
@@ -874,6 +907,7 @@ __global__ void __launch_bounds__(MINB == 1 ? 512 : 256, MINB) match_kernel(Matc
       }
       __syncwarp();
       last_change = global_ns();
+      busy_ns += last_change - t_item;
       continue;
     }
     unsigned int act = 0;
@@ -901,6 +935,9 @@ __global__ void __launch_bounds__(MINB == 1 ? 512 : 256, MINB) match_kernel(Matc
     __nanosleep(1000);
   }
   if (lane == 0) {
+    const unsigned long long t_end = global_ns();
+    atomicAdd(&a.stats[ST_WARP_NS], t_end - S.t_start);
+    atomicAdd(&a.stats[ST_IDLE_NS], t_end - t_drain - min(busy_ns, t_end - t_drain));
     atomicAdd(&a.stats[ST_SETOPS], w.setops);
     atomicAdd(&a.stats[ST_BYTES], w.bytes + 8ull * roots);
     atomicAdd(&a.stats[ST_ROOTS], roots);
@@ -1162,6 +1199,7 @@ void paged_release(pm_graph* g);
 pm_status paged_prepare(pm_ctx* ctx, pm_graph* g, bool cold, DPaging* out);
 pm_status paged_service_start(pm_ctx* ctx, pm_graph* g);
 pm_status paged_service_stop(pm_ctx* ctx, pm_graph* g, pm_stats* st);
+int64_t paged_static_frames(const pm_graph* g);
 }  // namespace pm
 
 extern "C" void pm_graph_opts_default(pm_graph_opts* o) {
@@ -1281,6 +1319,7 @@ extern "C" pm_status pm_graph_get_info(const pm_graph* g, pm_graph_info* info) {
   info->device_bytes = g->device_bytes;
   info->n_pages = (uint64_t)g->n_pages;
   info->n_frames = (uint64_t)g->n_frames;
+  info->n_static_frames = (uint64_t)paged_static_frames(g);
   return PM_OK;
 }
 
@@ -1625,6 +1664,8 @@ static pm_status finish_launch(const Launch& L, const unsigned long long* host_c
     so.page_misses = stt[ST_MISSES];
     so.zero_copy_bytes = stt[ST_ZC_BYTES];
     so.evictions = stt[ST_EVICTIONS];
+    so.warp_ns = stt[ST_WARP_NS];
+    so.idle_ns = stt[ST_IDLE_NS];
     so.kernel_ms = kernel_ms;
     so.roots_ms = roots_ms;
     so.grid_blocks = L.blocks;

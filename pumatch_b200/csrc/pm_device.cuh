@@ -42,7 +42,7 @@ struct DPlan {
 // power-of-two range of colidx; frames are page-sized slots of a device pool.
 struct DPaging {
   int32_t page_shift;              // log2(ints per page)
-  int32_t pad0;
+  int32_t n_static;                // frames [0, n_static) are never evicted or pinned
   int64_t n_pages;
   int64_t n_frames;
   int32_t* page_frame;             // [n_pages]: frame, or PAGE_ABSENT/LOADING/EVICTING

@@ -13,9 +13,11 @@
 //     table entry after it (same stream, so it lands after the data);
 //   * eviction is decided on the device (CLOCK over reference bits, skipping
 //     pinned frames), so the host never overwrites a frame a warp is reading.
+#include <algorithm>
 #include <atomic>
 #include <chrono>
 #include <cstring>
+#include <memory>
 #include <thread>
 #include <vector>
 
@@ -51,8 +53,13 @@ struct PagedState {
   unsigned int ring_slots = 1u << 16;
   int32_t* stage = nullptr;  // pinned: stage[f] = f, source of page-table publishes
   int64_t prefilled = 0;     // frames 0..prefilled-1 hold the initial resident pages
+  int64_t n_static = 0;      // frames 0..n_static-1 are never evicted (<= prefilled)
+  int64_t n_static_cap = 0;  // static frames the pool was created with
+  bool static_loaded = false;  // the static frames hold their pages already
   int32_t* init_pf = nullptr;  // pinned [n_pages]: page -> frame at the start of a run
   int32_t* init_fp = nullptr;  // pinned [n_frames]: frame -> page at the start of a run
+  int32_t* cold_pf = nullptr;  // pinned [n_pages]: the same for a cold run (static frames only)
+  int32_t* cold_fp = nullptr;  // pinned [n_frames]
   // service thread
   std::thread th;
   std::atomic<bool> stop{false};
@@ -76,41 +83,70 @@ static void release_state(PagedState* s) {
   cudaFreeHost(s->stage);
   cudaFreeHost(s->init_pf);
   cudaFreeHost(s->init_fp);
+  cudaFreeHost(s->cold_pf);
+  cudaFreeHost(s->cold_fp);
   if (s->copy_stream) cudaStreamDestroy(s->copy_stream);
   delete s;
 }
 
 // Resets the table to the initial residency (frames 0..prefilled-1 hold the
-// pages init_fp names), or to an empty pool when cold.  The initial pages are
-// (re)copied into their frames, since the last run may have evicted them.
+// pages init_fp names), or, when cold, to the static frames alone.  Evictable
+// initial pages are recopied into their frames every time, since the last run
+// may have evicted them; static frames are copied once.
 static pm_status reset_table(pm_graph* g, cudaStream_t st, bool cold) {
   PagedState* s = g->ps;
-  const int64_t pre = cold ? 0 : s->prefilled;
-  if (pre > 0) {
-    CKP(cudaMemcpyAsync(s->page_frame, s->init_pf, sizeof(int32_t) * g->n_pages, cudaMemcpyHostToDevice, st));
-    CKP(cudaMemcpyAsync(s->frame_page, s->init_fp, sizeof(int32_t) * g->n_frames, cudaMemcpyHostToDevice, st));
-    const size_t pb = (size_t)g->page_ints * 4;
-    for (int64_t f = 0; f < pre;) {
-      // coalesce runs of consecutive pages in consecutive frames into one copy
-      int64_t e = f + 1;
-      while (e < pre && s->init_fp[e] == s->init_fp[e - 1] + 1) e++;
-      const int64_t first = (int64_t)s->init_fp[f] * g->page_ints;
-      const size_t bytes = std::min<size_t>((size_t)(e - f) * pb, sizeof(int32_t) * (size_t)(g->nadj - first));
-      CKP(cudaMemcpyAsync((char*)s->frames + (size_t)f * pb, g->h_colidx + first, bytes, cudaMemcpyHostToDevice, st));
-      f = e;
-    }
-  } else {
-    CKP(cudaMemsetAsync(s->page_frame, 0xff, sizeof(int32_t) * g->n_pages, st));  // PAGE_ABSENT
-    CKP(cudaMemsetAsync(s->frame_page, 0xff, sizeof(int32_t) * g->n_frames, st));
+  const int64_t pre = cold ? s->n_static : s->prefilled;
+  const int32_t* pf = cold ? s->cold_pf : s->init_pf;
+  const int32_t* fp = cold ? s->cold_fp : s->init_fp;
+  CKP(cudaMemcpyAsync(s->page_frame, pf, sizeof(int32_t) * g->n_pages, cudaMemcpyHostToDevice, st));
+  CKP(cudaMemcpyAsync(s->frame_page, fp, sizeof(int32_t) * g->n_frames, cudaMemcpyHostToDevice, st));
+  const size_t pb = (size_t)g->page_ints * 4;
+  for (int64_t f = s->static_loaded ? s->n_static : 0; f < pre;) {
+    // coalesce runs of consecutive pages in consecutive frames into one copy
+    // (a run never crosses the static boundary)
+    int64_t e = f + 1;
+    while (e < pre && e != s->n_static && fp[e] == fp[e - 1] + 1) e++;
+    const int64_t first = (int64_t)fp[f] * g->page_ints;
+    const size_t bytes = std::min<size_t>((size_t)(e - f) * pb, sizeof(int32_t) * (size_t)(g->nadj - first));
+    CKP(cudaMemcpyAsync((char*)s->frames + (size_t)f * pb, g->h_colidx + first, bytes, cudaMemcpyHostToDevice, st));
+    f = e;
   }
   CKP(cudaMemsetAsync(s->frame_pin, 0, sizeof(int32_t) * g->n_frames, st));
   CKP(cudaMemsetAsync(s->frame_ref, 0, g->n_frames, st));
   unsigned long long h[4] = {0, (unsigned long long)pre, 0, 0};
   CKP(cudaMemcpyAsync(s->dctl, h, sizeof(h), cudaMemcpyHostToDevice, st));
   CKP(cudaStreamSynchronize(st));
+  s->static_loaded = true;
   s->tail = 0;
   *(volatile unsigned long long*)s->host_tail = 0;
   memset(s->ring_seq, 0, sizeof(unsigned long long) * s->ring_slots);
+  return PM_OK;
+}
+
+// Fills init_* / cold_* from a page list: the first n_static entries, sorted,
+// take the static frames; the rest, in the given order, the evictable ones.
+static pm_status set_initial(pm_graph* g, std::vector<int64_t> pages) {
+  PagedState* s = g->ps;
+  const int64_t k = std::min<int64_t>((int64_t)pages.size(), g->n_frames);
+  pages.resize((size_t)k);
+  std::vector<int32_t> pf((size_t)g->n_pages, PAGE_ABSENT);
+  for (int64_t f = 0; f < k; f++) {
+    if (pages[f] < 0 || pages[f] >= g->n_pages) return fail(PM_ERR_INVALID, "page %lld out of range", (long long)pages[f]);
+    if (pf[pages[f]] != PAGE_ABSENT) return fail(PM_ERR_INVALID, "page %lld listed twice", (long long)pages[f]);
+    pf[pages[f]] = 0;
+  }
+  const int64_t ns = std::min<int64_t>(s->n_static, k);
+  std::sort(pages.begin(), pages.begin() + ns);
+  for (int64_t p = 0; p < g->n_pages; p++) s->init_pf[p] = s->cold_pf[p] = PAGE_ABSENT;
+  for (int64_t f = 0; f < g->n_frames; f++) {
+    s->init_fp[f] = f < k ? (int32_t)pages[f] : -1;
+    s->cold_fp[f] = f < ns ? (int32_t)pages[f] : -1;
+    if (f < k) s->init_pf[pages[f]] = (int32_t)f;
+    if (f < ns) s->cold_pf[pages[f]] = (int32_t)f;
+  }
+  s->prefilled = k;
+  s->n_static = ns;
+  s->static_loaded = false;
   return PM_OK;
 }
 
@@ -160,14 +196,22 @@ pm_status paged_place(pm_graph* g, const int32_t* colidx, const pm_graph_opts* o
   CKP(cudaStreamCreateWithFlags(&s->copy_stream, cudaStreamNonBlocking));
   // warm start: the first pages of the array, the way the reference keeps the
   // first 60% of the edges on the device (test.cu:22-43)
-  CKP(cudaHostAlloc((void**)&s->init_pf, sizeof(int32_t) * std::max<int64_t>(g->n_pages, 1), cudaHostAllocPortable));
-  CKP(cudaHostAlloc((void**)&s->init_fp, sizeof(int32_t) * std::max<int64_t>(g->n_frames, 1), cudaHostAllocPortable));
-  s->prefilled = g->n_frames;
-  for (int64_t p = 0; p < g->n_pages; p++) s->init_pf[p] = p < g->n_frames ? (int32_t)p : PAGE_ABSENT;
-  for (int64_t f = 0; f < g->n_frames; f++) s->init_fp[f] = (int32_t)f;
+  const size_t pfb = sizeof(int32_t) * std::max<int64_t>(g->n_pages, 1);
+  const size_t fpb = sizeof(int32_t) * std::max<int64_t>(g->n_frames, 1);
+  CKP(cudaHostAlloc((void**)&s->init_pf, pfb, cudaHostAllocPortable));
+  CKP(cudaHostAlloc((void**)&s->init_fp, fpb, cudaHostAllocPortable));
+  CKP(cudaHostAlloc((void**)&s->cold_pf, pfb, cudaHostAllocPortable));
+  CKP(cudaHostAlloc((void**)&s->cold_fp, fpb, cudaHostAllocPortable));
+  s->n_static = s->n_static_cap = std::min<int64_t>((int64_t)(o->static_pool_bytes / pb), g->n_frames);
   g->ps = s.release();
+  std::vector<int64_t> prefix((size_t)g->n_frames);
+  for (int64_t f = 0; f < g->n_frames; f++) prefix[f] = f;
+  pm_status st = set_initial(g, std::move(prefix));
+  if (st != PM_OK) return st;
   return reset_table(g, g->ps->copy_stream, false);
 }
+
+int64_t paged_static_frames(const pm_graph* g) { return g->ps ? g->ps->n_static : 0; }
 
 pm_status paged_maxnbrdeg(pm_graph* g) { return compute_maxnbrdeg(g, g->h_colidx_dev); }
 
@@ -194,6 +238,7 @@ pm_status paged_prepare(pm_ctx* c, pm_graph* g, bool cold, DPaging* out) {
   int shift = 0;
   while ((1u << shift) < g->page_ints) shift++;
   out->page_shift = shift;
+  out->n_static = (int32_t)s->n_static;
   out->n_pages = g->n_pages;
   out->n_frames = g->n_frames;
   out->page_frame = s->page_frame;
@@ -281,23 +326,19 @@ pm_status paged_service_stop(pm_ctx* c, pm_graph* g, pm_stats* st) {
 }  // namespace pm
 
 // Chooses the pages the frame pool starts each (non-cold) run with -- e.g.
-// the pages a cost model predicts the hottest.  Pages beyond the pool size
-// are ignored; duplicates are an error.
+// the pages a cost model predicts the hottest.  The first n_static_frames of
+// the list become the static (never evicted) pages; pages beyond the pool
+// size are ignored; duplicates are an error.
 extern "C" pm_status pm_graph_set_resident_pages(pm_graph* g, const int64_t* pages, int64_t n) {
   using namespace pm;
   if (!g || (n > 0 && !pages) || n < 0) return fail(PM_ERR_INVALID, "pm_graph_set_resident_pages: bad arguments");
   if (g->residency != PM_RESIDENT_PAGED || !g->ps) return fail(PM_ERR_INVALID, "graph is not paged");
-  PagedState* s = g->ps;
   CKP(cudaSetDevice(g->device));
-  const int64_t k = std::min<int64_t>(n, g->n_frames);
-  std::vector<int32_t> pf((size_t)g->n_pages, PAGE_ABSENT);
-  for (int64_t f = 0; f < k; f++) {
-    if (pages[f] < 0 || pages[f] >= g->n_pages) return fail(PM_ERR_INVALID, "page %lld out of range", (long long)pages[f]);
-    if (pf[pages[f]] != PAGE_ABSENT) return fail(PM_ERR_INVALID, "page %lld listed twice", (long long)pages[f]);
-    pf[pages[f]] = (int32_t)f;
-  }
-  memcpy(s->init_pf, pf.data(), sizeof(int32_t) * g->n_pages);
-  for (int64_t f = 0; f < g->n_frames; f++) s->init_fp[f] = f < k ? (int32_t)pages[f] : -1;
-  s->prefilled = k;
-  return PM_OK;
+  // the static count is the pool's, not the list's: keep it across calls
+  PagedState* s = g->ps;
+  const int64_t before = s->n_static;
+  s->n_static = s->n_static_cap;
+  pm_status st = set_initial(g, std::vector<int64_t>(pages, pages + n));
+  if (st != PM_OK) s->n_static = before;
+  return st;
 }

@@ -56,6 +56,7 @@ __device__ __forceinline__ void ring_post(const DPaging& pg, unsigned long long 
 // claim the page, find a frame (never-used frames first, then a bounded
 // CLOCK sweep), post the request.  Never waits for the host.
 static __device__ void request_page(const DPaging& pg, int32_t p, PageCounters& pc) {
+  if (pg.n_static >= pg.n_frames) return;  // no evictable frame to load into
   if (ld_vol(&pg.page_frame[p]) != PAGE_ABSENT) return;
   const unsigned long long slot = ring_reserve(pg);
   if (slot == ~0ull) { pc.dropped++; return; }
@@ -65,12 +66,13 @@ static __device__ void request_page(const DPaging& pg, int32_t p, PageCounters& 
   }
   int32_t f = -1;
   const unsigned long long k = atomicAdd(pg.next_free, 1ull);
+  const int64_t n_dyn = pg.n_frames - pg.n_static;  // evictable frames
   if (k < (unsigned long long)pg.n_frames) {
     f = (int32_t)k;
-  } else {
-    const int sweep = (int)min((int64_t)4096, 2 * pg.n_frames + 8);  // bounded CLOCK sweep
+  } else if (n_dyn > 0) {
+    const int sweep = (int)min((int64_t)4096, 2 * n_dyn + 8);  // bounded CLOCK sweep
     for (int t = 0; t < sweep && f < 0; t++) {
-      const int32_t h = (int32_t)(atomicAdd(pg.clock_hand, 1ull) % (unsigned long long)pg.n_frames);
+      const int32_t h = pg.n_static + (int32_t)(atomicAdd(pg.clock_hand, 1ull) % (unsigned long long)n_dyn);
       if (pg.frame_ref[h]) { pg.frame_ref[h] = 0; continue; }
       if (ld_vol(&pg.frame_pin[h]) != 0) continue;
       const int32_t q = ld_vol(&pg.frame_page[h]);
@@ -98,9 +100,11 @@ static __device__ void request_page(const DPaging& pg, int32_t p, PageCounters& 
 }
 
 // Pins the frame holding page p if it is resident; returns the frame or -1.
+// A static frame is returned as is: its entry never changes during a run.
 __device__ __forceinline__ int32_t try_pin(const DPaging& pg, int32_t p) {
   const int32_t f = ld_vol(&pg.page_frame[p]);
   if (f < 0) return -1;
+  if (f < pg.n_static) return f;
   atomicAdd(&pg.frame_pin[f], 1);
   __threadfence();
   if (ld_vol(&pg.page_frame[p]) != f) {
@@ -109,6 +113,20 @@ __device__ __forceinline__ int32_t try_pin(const DPaging& pg, int32_t p) {
   }
   pg.frame_ref[f] = 1;
   return f;
+}
+
+__device__ __forceinline__ void unpin_frame(const DPaging& pg, int32_t f) {
+  if (f >= pg.n_static) atomicSub(&pg.frame_pin[f], 1);
+}
+
+// Frame of page p0 when pages p0..p1 all sit in consecutive static frames (a
+// list over them can be read in place), else -1.
+__device__ __forceinline__ int32_t static_run(const DPaging& pg, int32_t p0, int32_t p1) {
+  const int32_t f0 = ld_vol(&pg.page_frame[p0]);
+  if (f0 < 0 || f0 + (p1 - p0) >= pg.n_static) return -1;
+  for (int32_t k = p0 + 1; k <= p1; k++)
+    if (ld_vol(&pg.page_frame[k]) != f0 + (k - p0)) return -1;
+  return f0;
 }
 
 struct ListRef {
@@ -140,6 +158,8 @@ static __device__ ListRef paged_list(const DPaging& pg, uint64_t b, int len, int
       f0 = try_pin(pg, p0);
       if (f0 >= 0) mode = 0;
       else request_page(pg, p0, pc);
+    } else if ((f0 = static_run(pg, p0, p1)) >= 0) {
+      mode = 0;  // contiguous in the static frames: read in place, no pins
     } else if (p1 - p0 < PM_MAX_LIST_PAGES) {
       int32_t k = p0;
       for (; k <= p1; k++) {
@@ -150,7 +170,7 @@ static __device__ ListRef paged_list(const DPaging& pg, uint64_t b, int len, int
       if (k > p1) {
         mode = 2;
       } else {
-        for (int32_t j = p0; j < k; j++) atomicSub(&pg.frame_pin[pins[j - p0]], 1);
+        for (int32_t j = p0; j < k; j++) unpin_frame(pg, pins[j - p0]);
         for (int32_t j = p0, posted = 0; j <= p1 && posted < 4; j++)
           if (ld_vol(&pg.page_frame[j]) == PAGE_ABSENT) { request_page(pg, j, pc); posted++; }
       }
@@ -177,13 +197,13 @@ static __device__ ListRef paged_list(const DPaging& pg, uint64_t b, int len, int
   }
   __syncwarp();
   if (lane == 0)
-    for (int32_t k = p0; k <= p1; k++) atomicSub(&pg.frame_pin[pins[k - p0]], 1);
+    for (int32_t k = p0; k <= p1; k++) unpin_frame(pg, pins[k - p0]);
   __syncwarp();
   return ListRef{gather, len, -1};
 }
 
 __device__ __forceinline__ void unpin(const DPaging& pg, const ListRef& r) {
-  if (r.pinned >= 0 && (threadIdx.x & 31) == 0) atomicSub(&pg.frame_pin[r.pinned], 1);
+  if (r.pinned >= 0 && (threadIdx.x & 31) == 0) unpin_frame(pg, r.pinned);
 }
 
 }  // namespace pm

@@ -64,6 +64,39 @@ def test_paged_counts_exact(ctx, page_kb, frames):
         g.close()
 
 
+@pytest.mark.parametrize("page_kb,frames,static", [(4, 16, 8), (4, 200, 150), (16, 8, 8), (4, 64, 1), (64, 10000, 10000)])
+def test_paged_static_frames_exact(ctx, page_kb, frames, static):
+    """Part of the pool placed once and never evicted (the reference's device
+    partition): counts stay exact warm and cold, with and without spare frames."""
+    hg = workload()
+    pb = page_kb << 10
+    for labeled in (True, False):
+        g = pm.GraphPreprocessor.from_host(hg, labeled=labeled, paged=True, page_bytes=pb,
+                                           frame_pool_bytes=frames * pb, static_pool_bytes=static * pb)
+        info = g.info()
+        assert info["n_static_frames"] == min(static, info["n_frames"])
+        for name, (text, lab) in TEXTS.items():
+            if lab != labeled:
+                continue
+            want, ost = oracle(hg, name)
+            p = pm.PatternPreprocessor(text=text, labeled=labeled)
+            for cold in (True, False, True):
+                got, st = ctx.match(g, [p], cold_cache=cold, timeout_ms=120000)
+                assert got[0] == want, (name, page_kb, frames, static, cold)
+                assert st["set_ops"] == ost["set_ops"]
+                assert st["device_status"] == 0
+        if info["n_pages"] > 2:
+            # learned-style residency: a scattered page set, static part sorted
+            pages = list(range(info["n_pages"] - 1, -1, -3))
+            g.set_resident_pages(pages)
+            assert g.info()["n_static_frames"] == min(static, info["n_frames"], len(pages))
+            for name, (text, lab) in TEXTS.items():
+                if lab == labeled:
+                    got, _ = ctx.match(g, [pm.PatternPreprocessor(text=text, labeled=labeled)])
+                    assert got[0] == oracle(hg, name)[0]
+        g.close()
+
+
 def test_paged_pressure_evicts_and_loads(ctx):
     hg = workload()
     g = pm.GraphPreprocessor.from_host(hg, labeled=True, paged=True, page_bytes=4096, frame_pool_bytes=32 * 4096)
