@@ -365,7 +365,18 @@ def run_ours(args, workload):
                          "alg_bytes_per_launch": int(per_launch_bytes)},
             "gpu_launches": launches,
             "clocks": clk.summary(),
+            "warp_idle_frac_last_step": st["idle_ns"] / max(1, st["warp_ns"]),
         }
+        if w.get("paged"):
+            info = graph.info()
+            link = st["h2d_page_bytes"] + st["zero_copy_bytes"]
+            line["host_link"] = {
+                "pages": int(info["n_pages"]), "frames": int(info["n_frames"]),
+                "static_frames": int(info["n_static_frames"]), "page_bytes": w["paged"]["page_bytes"],
+                "page_hits_last_step": int(st["page_hits"]), "h2d_page_bytes_last_step": int(st["h2d_page_bytes"]),
+                "zero_copy_bytes_last_step": int(st["zero_copy_bytes"]),
+                "achieved_gbs": link / (st["kernel_ms"] / 1000.0) / 1e9 if st["kernel_ms"] > 0 else 0.0,
+                "nominal_gbs": 64.0, "nominal": "PCIe Gen5 x16, one direction"}
         if world == 1 and not args.no_cpu_baseline:
             threads = os.cpu_count() or 1
             m, dt, n_s, n_tot = cpu_sample_run(hg, texts, labeled, threads, target_s=15.0)

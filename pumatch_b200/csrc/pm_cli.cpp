@@ -2,6 +2,7 @@
 //
 //   test <graph-prefix> <pattern.g> [--labeled=0|1] [--truncate=N] [--device=D]
 //        [--paged] [--frame-mb=M] [--static-mb=S] [--page-kb=K] [--batch=<list file>]
+//        [--warps=W] [--chunk=C] [--split=S] [--tuned=<autotuner json>]
 //
 // Same positional arguments and output as the reference's driver
 // (test.cu:15-21, 200-209): the last stdout line is "<kernel ms> <count>" and
@@ -12,15 +13,36 @@
 // With --batch, <pattern.g> is ignored and each line of the list file names a
 // pattern; all run in one launch and one "<ms> <count>" line is printed per
 // pattern in list order (ms is the shared launch time).
+// --tuned reads the "best" record the autotuner writes (warps_per_block,
+// chunk, split_level1, page_kb); explicit flags after it override it.
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <fstream>
 #include <iostream>
+#include <iterator>
 #include <string>
 #include <vector>
 
 #include "pumatch.h"
+
+// Integer value of "key" in the first JSON object that follows "best" (the
+// autotuner's output); false when absent or null.
+static bool tuned_int(const std::string& text, const char* key, long long* out) {
+  size_t at = text.find("\"best\"");
+  if (at == std::string::npos) return false;
+  const size_t end = text.find('}', at);
+  const std::string k = std::string("\"") + key + "\"";
+  size_t p = text.find(k, at);
+  if (p == std::string::npos || (end != std::string::npos && p > end)) return false;
+  p = text.find(':', p + k.size());
+  if (p == std::string::npos) return false;
+  char* e = nullptr;
+  const long long v = strtoll(text.c_str() + p + 1, &e, 10);
+  if (e == text.c_str() + p + 1) return false;
+  *out = v;
+  return true;
+}
 
 static int die(const char* what, pm_status s) {
   fprintf(stderr, "test: %s: %s (%s)\n", what, pm_strerror(s), pm_last_error());
@@ -30,17 +52,33 @@ static int die(const char* what, pm_status s) {
 int main(int argc, char** argv) {
   if (argc < 3) {
     fprintf(stderr, "usage: test <graph-prefix> <pattern.g> [--labeled=0|1] [--truncate=N] [--device=D]\n"
-                    "            [--paged] [--frame-mb=M] [--static-mb=S] [--page-kb=K] [--batch=<list>]\n");
+                    "            [--paged] [--frame-mb=M] [--static-mb=S] [--page-kb=K] [--batch=<list>]\n"
+                    "            [--warps=W] [--chunk=C] [--split=S] [--tuned=<json>]\n");
     return 2;
   }
   const char* prefix = argv[1];
   std::string pattern = argv[2];
   int labeled = 1, truncate = 0, device = 0, paged = 0;
   long long frame_mb = 4096, static_mb = 0, page_kb = 64;
+  long long warps = 0, chunk = 0, split = 0;
   std::string batch;
   for (int i = 3; i < argc; i++) {
     const char* a = argv[i];
-    if (!strncmp(a, "--labeled=", 10)) labeled = atoi(a + 10);
+    if (!strncmp(a, "--tuned=", 8)) {
+      std::ifstream f(a + 8);
+      if (!f.good()) { fprintf(stderr, "test: cannot open %s\n", a + 8); return 1; }
+      const std::string text((std::istreambuf_iterator<char>(f)), std::istreambuf_iterator<char>());
+      long long v;
+      if (text.find("\"best\"") == std::string::npos) { fprintf(stderr, "test: %s has no \"best\" record\n", a + 8); return 1; }
+      if (tuned_int(text, "warps_per_block", &v)) warps = v;
+      if (tuned_int(text, "chunk", &v)) chunk = v;
+      if (tuned_int(text, "split_level1", &v)) split = v;
+      if (tuned_int(text, "page_kb", &v)) page_kb = v;
+    }
+    else if (!strncmp(a, "--warps=", 8)) warps = atoll(a + 8);
+    else if (!strncmp(a, "--chunk=", 8)) chunk = atoll(a + 8);
+    else if (!strncmp(a, "--split=", 8)) split = atoll(a + 8);
+    else if (!strncmp(a, "--labeled=", 10)) labeled = atoi(a + 10);
     else if (!strncmp(a, "--truncate=", 11)) truncate = atoi(a + 11);
     else if (!strncmp(a, "--device=", 9)) device = atoi(a + 9);
     else if (!strcmp(a, "--paged")) paged = 1;
@@ -92,6 +130,9 @@ int main(int argc, char** argv) {
   pm_run_opts ro;
   pm_run_opts_default(&ro);
   ro.truncate = truncate;
+  if (warps) ro.warps_per_block = (int32_t)warps;
+  if (chunk) ro.chunk = (int32_t)chunk;
+  if (split) ro.split_level1 = (int32_t)split;
   std::vector<uint64_t> counts(plans.size(), 0);
   pm_stats st;
   s = pm_match(ctx, g, plans.data(), (int)plans.size(), &ro, counts.data(), &st);

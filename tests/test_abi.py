@@ -92,3 +92,17 @@ def test_no_cpu_fallback():
 def test_cli_usage():
     r = subprocess.run([pm.CLI_PATH], capture_output=True, text=True)
     assert r.returncode == 2 and "usage" in r.stderr
+    assert "--tuned" in r.stderr
+
+
+def test_cli_tuned_file_errors(tmp_path):
+    gold = os.path.join(ROOT, "tests", "golden", "graphs", "cl400")
+    r = subprocess.run([pm.CLI_PATH, gold, "x.g", "--tuned=" + str(tmp_path / "none.json")],
+                       capture_output=True, text=True)
+    assert r.returncode == 1 and "cannot open" in r.stderr
+    bad = tmp_path / "bad.json"
+    bad.write_text('{"results": []}')
+    r = subprocess.run([pm.CLI_PATH, gold, "x.g", "--tuned=" + str(bad)], capture_output=True, text=True)
+    assert r.returncode == 1 and "best" in r.stderr
+    r = subprocess.run([pm.CLI_PATH, gold, "x.g", "--bogus"], capture_output=True, text=True)
+    assert r.returncode == 2

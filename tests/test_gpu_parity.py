@@ -239,6 +239,15 @@ def test_gpu_cli_output(tmp_path):
     assert r.returncode == 0, r.stderr
     want, _ = oracle_count(host_graph("cl400", False), PATTERNS["cycle5_lab"], False, truncate=8)
     assert int(r.stdout.strip().splitlines()[-1].split()[1]) == want
+    # launch configuration from an autotuner record, then overridden by a flag
+    tuned = tmp_path / "tuned.json"
+    tuned.write_text('{"best": {"warps_per_block": 4, "chunk": 32, "split_level1": 16, "page_kb": null, '
+                     '"kernel_ms": 1.0}, "results": []}')
+    r = subprocess.run([pm.CLI_PATH, prefix, str(pat), "--tuned=" + str(tuned), "--chunk=8"], capture_output=True,
+                       text=True, cwd=tmp_path)
+    assert r.returncode == 0, r.stderr
+    want, _ = oracle_count(host_graph("cl400", True), PATTERNS["cycle5_lab"], True)
+    assert int(r.stdout.strip().splitlines()[-1].split()[1]) == want
 
 
 REF_COUNTS = os.path.join(GOLD, "ref_gpu_counts.json")
