@@ -495,14 +495,17 @@ def run_batch_compare(args, workload):
             "counts": c, "batched_ms": statistics.median(batched), "graph_replay_kernel_ms": statistics.median(replay),
             "sequential_ms": statistics.median(seq),
             "speedup": statistics.median(seq) / statistics.median(batched)}
+    print(json.dumps(line), flush=True)
     if args.autotune:
         from pumatch_b200 import autotune
+        limit = max(10.0, 3.0 * statistics.median(batched) / 1000.0)  # a config 3x slower is not a candidate
         rows = autotune.sweep(ctx, g, plans, warps=(4, 8, 16), chunks=(32, 256, 2048), splits=(16, 64),
-                              timeout_ms=args.timeout_s * 1000)
-        best = min(rows, key=lambda r: r["kernel_ms"])
-        line["autotune"] = {"best": best, "default_kernel_ms": statistics.median(batched), "configs": len(rows),
-                            "results": rows}
-    print(json.dumps(line), flush=True)
+                              timeout_ms=int(limit * 1000))
+        done = [r for r in rows if r["kernel_ms"] is not None]
+        best = min(done, key=lambda r: r["kernel_ms"]) if done else None
+        tuned = {"metric": "autotune_batched_ms", "workload": workload, "best": best,
+                 "default_kernel_ms": statistics.median(batched), "configs": len(rows), "results": rows}
+        print(json.dumps(tuned), flush=True)
 
 
 def main():

@@ -208,9 +208,11 @@ typedef struct {
   int32_t warps_per_block;  /* 0 = default                                  */
   int32_t blocks_per_sm;    /* 0 = default                                  */
   int32_t chunk;            /* root edges per queue pop; 0 = default         */
-  int32_t split_level1;     /* >0: donate level-1 ranges of at least this
-                               many candidates to idle warps; 0 = default;
-                               -1 = never split                              */
+  int32_t split_level1;     /* work donation to idle warps: >0 = a range of
+                               candidates that only lead to the last level
+                               is donated from this length on (ranges heading
+                               deeper subtrees from 2 on); 0 = default (64);
+                               -1 = never donate                             */
   int32_t shard_rank;       /* multi-GPU root sharding: this shard (0-based) */
   int32_t shard_count;      /* number of shards; 0/1 = no sharding; shard k
                                takes root chunks k, k+count, ...            */

@@ -16,7 +16,7 @@ import json
 import time
 from typing import Callable, Dict, Iterable, List, Optional, Sequence
 
-from . import Context, GraphPreprocessor, HostGraph, PatternPreprocessor
+from . import PM_ERR_TIMEOUT, Context, GraphPreprocessor, HostGraph, PatternPreprocessor, PmError
 
 WARPS = (4, 8, 16)
 CHUNKS = (32, 64, 128, 256, 512, 1024, 2048, 4096)
@@ -34,8 +34,13 @@ def sweep(ctx: Context, graph: GraphPreprocessor, plans: Sequence[PatternPreproc
     for w, c, s in itertools.product(warps, chunks, splits):
         best = None
         for _ in range(reps):
-            counts, st = ctx.match(graph, list(plans), warps_per_block=w, chunk=c, split_level1=s,
-                                   timeout_ms=timeout_ms, **extra)
+            try:
+                counts, st = ctx.match(graph, list(plans), warps_per_block=w, chunk=c, split_level1=s,
+                                       timeout_ms=timeout_ms, **extra)
+            except PmError as e:
+                if e.status != PM_ERR_TIMEOUT:
+                    raise
+                break  # slower than the limit: not a candidate (kernel_ms stays None)
             if want is None:
                 want = counts
             if counts != want:
@@ -62,7 +67,10 @@ def autotune(ctx: Context, hg: HostGraph, plans: Sequence[PatternPreprocessor], 
                 results.append(r)
         finally:
             g.close()
-    best = min(results, key=lambda r: r["kernel_ms"])
+    done = [r for r in results if r["kernel_ms"] is not None]
+    if not done:
+        raise RuntimeError("every configuration hit the time limit")
+    best = min(done, key=lambda r: r["kernel_ms"])
     out = {"best": best, "results": results, "when": time.strftime("%Y-%m-%dT%H:%M:%SZ", time.gmtime())}
     if out_json:
         with open(out_json, "w") as f:

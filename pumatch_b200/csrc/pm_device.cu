@@ -74,7 +74,8 @@ struct MatchArgs {
   const int32_t* colidx;        // HBM residency
   const uint8_t* labels;
   const int32_t* colidx_lab;    // label-grouped lists (labeled, HBM) or null
-  const int32_t* lab_off;
+  const int32_t* lab_off;       // label group offsets (labeled, HBM or paged) or null
+  const int32_t* host_sorted;   // labeled paged: the id-sorted lists in mapped host memory
   int32_t nl1;
   int32_t pad1;
   int32_t n;
@@ -83,7 +84,7 @@ struct MatchArgs {
   int32_t chunk;
   int32_t shard_rank;
   int32_t shard_count;
-  int32_t split_min;            // donate level-1 ranges at least this long
+  int32_t split_min;            // donate last-but-one-level ranges at least this long
   int32_t maxdeg;
   unsigned long long* cursors;  // [nplans]
   unsigned long long* counts;   // [nplans]
@@ -138,22 +139,23 @@ struct Work {
   PageCounters pc;
 };
 
+// CG: the list may sit in an evictable frame; cg: it does (runtime).
 template <bool CG>
-__device__ __forceinline__ int32_t ld(const int32_t* p) {
-  if (CG) return __ldcg(p);  // frames are refilled during the launch: skip L1
+__device__ __forceinline__ int32_t ld(const int32_t* p, bool cg = true) {
+  if (CG && cg) return __ldcg(p);  // evictable frames are refilled during the launch: skip L1
   return *p;
 }
 
 // First index of sorted A[0,len) whose element is >= ub: a 32-ary search,
 // one strided probe per lane per round (log32(len) rounds).
 template <bool CG>
-__device__ __forceinline__ int warp_lower_bound(const int32_t* A, int len, int ub) {
+__device__ __forceinline__ int warp_lower_bound(const int32_t* A, int len, int ub, bool cg = true) {
   const int lane = lane_id();
   int lo = 0, hi = len;
   while (hi - lo > 32) {
     const int step = (hi - lo + 31) >> 5;
     const long long idx = lo + (long long)lane * step;
-    const bool lt = idx < hi && ld<CG>(A + idx) < ub;
+    const bool lt = idx < hi && ld<CG>(A + idx, cg) < ub;
     const int k = __popc(__ballot_sync(FULL, lt));
     if (k == 0) return lo;
     const int nhi = min(hi, lo + k * step);
@@ -161,40 +163,54 @@ __device__ __forceinline__ int warp_lower_bound(const int32_t* A, int len, int u
     hi = nhi;
   }
   const int idx = lo + lane;
-  const bool lt = idx < hi && ld<CG>(A + idx) < ub;
+  const bool lt = idx < hi && ld<CG>(A + idx, cg) < ub;
   return lo + __popc(__ballot_sync(FULL, lt));
 }
 
 // Membership of x in sorted B[0, len) by binary search (per lane).
 template <bool CG>
-__device__ __forceinline__ bool bsearch_in(const int32_t* B, int len, int x) {
+__device__ __forceinline__ bool bsearch_in(const int32_t* B, int len, int x, bool cg = true) {
   int lo = 0, hi = len;
   while (lo < hi) {
     const int mid = (lo + hi) >> 1;
-    if (ld<CG>(B + mid) < x) lo = mid + 1; else hi = mid;
+    if (ld<CG>(B + mid, cg) < x) lo = mid + 1; else hi = mid;
   }
-  return lo < len && ld<CG>(B + lo) == x;
+  return lo < len && ld<CG>(B + lo, cg) == x;
 }
 
-// Adjacency list of v: a slice of colidx in HBM, or resolved through the
-// page cache (frame, gathered copy, or host read).
+// Adjacency list of v in id order: a slice of colidx in HBM, or resolved
+// through the page cache (frame, gathered copy, or host read).  A labeled
+// paged graph caches its label-grouped copy, so its whole sorted lists are
+// read from host memory.
 template <bool PAGED>
 __device__ __forceinline__ ListRef adj(const MatchArgs& a, WarpState& S, int v, int32_t* gather, Work& w) {
   const uint64_t b = a.rowptr[v];
   const int len = (int)(a.rowptr[v + 1] - b);
   w.reads++;
   if (!PAGED) return ListRef{a.colidx + b, len, -1};
+  if (a.host_sorted) return ListRef{a.host_sorted + b, len, -1};
   return paged_list(a.pg, b, len, gather, S.pins, w.pc);
 }
 
-// The label-l part of v's list (labeled graphs in HBM), in id order; empty
-// for a label no vertex of the graph carries.
-__device__ __forceinline__ ListRef adj_label(const MatchArgs& a, int v, int l) {
-  const uint64_t b = a.rowptr[v];
-  if (l >= a.nl1 - 1) return ListRef{a.colidx_lab + b, 0, -1};
+// Start (relative to v's list) and length of the label-l part of v's list;
+// empty for a label no vertex of the graph carries.
+__device__ __forceinline__ int2 label_range(const MatchArgs& a, int v, int l) {
+  if (l >= a.nl1 - 1) return make_int2(0, 0);
   const int32_t* o = a.lab_off + (int64_t)v * a.nl1;
-  const int s0 = o[l], s1 = o[l + 1];
-  return ListRef{a.colidx_lab + b + s0, s1 - s0, -1};
+  const int s0 = o[l];
+  return make_int2(s0, o[l + 1] - s0);
+}
+
+// The label-l part of v's list, in id order: from the grouped copy in HBM,
+// or through the page cache over the grouped copy.
+template <bool PAGED>
+__device__ __forceinline__ ListRef adj_label(const MatchArgs& a, WarpState& S, int v, int l, int32_t* gather,
+                                             Work& w) {
+  const uint64_t b = a.rowptr[v];
+  const int2 r = label_range(a, v, l);
+  w.reads++;
+  if (!PAGED) return ListRef{a.colidx_lab + b + r.x, r.y, -1};
+  return paged_list(a.pg, b + (uint64_t)r.x, r.y, gather, S.pins, w.pc);
 }
 
 // ---------------------------------------------------------------------
@@ -216,13 +232,13 @@ __device__ int run_slot(const MatchArgs& a, const DPlan& P, WarpState& S, int32_
   // survivors in the same order, no label gathers (accounting still charges
   // the whole list, as the reference scans it)
   const uint32_t mask0 = P.slot_labels[s];
-  const bool by_label = LABELED && !PAGED && a.colidx_lab && __popc(mask0) == 1 && (kind != SLOT_COPY || L == 1);
+  const bool by_label = LABELED && a.lab_off && __popc(mask0) == 1 && (kind != SLOT_COPY || L == 1);
   int full_len = -1;  // length of the whole list when by_label
+  int full_lenB = -1; // the same for a level-1 second operand read by label (paged)
   if (by_label) {
     const int v = (kind != SLOT_COPY) ? vL : S.path[0];
     full_len = (int)(a.rowptr[v + 1] - a.rowptr[v]);
-    RA = adj_label(a, v, __ffs(mask0) - 1);
-    w.reads++;
+    RA = adj_label<PAGED>(a, S, v, __ffs(mask0) - 1, gatherA, w);
   } else if (kind != SLOT_COPY) {
     RA = adj<PAGED>(a, S, vL, gatherA, w);
   } else if (L > 1) {
@@ -231,19 +247,30 @@ __device__ int run_slot(const MatchArgs& a, const DPlan& P, WarpState& S, int32_
     RA = adj<PAGED>(a, S, S.path[0], gatherA, w);
   }
   if (kind == SLOT_INTERSECT) {
-    if (L > 1) RB = ListRef{arena + S.off[P.parent[s]], S.size[P.parent[s]], -1};
-    else RB = adj<PAGED>(a, S, S.path[0], gatherB, w);
+    if (L > 1) {
+      RB = ListRef{arena + S.off[P.parent[s]], S.size[P.parent[s]], -1};
+    } else if (PAGED && by_label) {
+      // only the label-l part of N(v0) can meet the label-l part of N(vL)
+      const int v0 = S.path[0];
+      full_lenB = (int)(a.rowptr[v0 + 1] - a.rowptr[v0]);
+      RB = adj_label<PAGED>(a, S, v0, __ffs(mask0) - 1, gatherB, w);
+    } else {
+      RB = adj<PAGED>(a, S, S.path[0], gatherB, w);
+    }
   }
   const int32_t* A = RA.p;
   const int32_t* B = RB.p;
   int lenA = RA.len;
   const int lenB = RB.len;
+  const bool cgA = RA.cg;
+  bool cgB = RB.cg;
   // a parent slot small enough goes to shared memory for the per-lane searches
-  if (kind == SLOT_INTERSECT && L > 1 && lenB <= PM_SB_MAX && !PAGED) {
+  if (kind == SLOT_INTERSECT && L > 1 && lenB <= PM_SB_MAX) {
     __syncwarp();
     for (int i = lane; i < lenB; i += 32) S.sb[i] = B[i];
     __syncwarp();
     B = S.sb;
+    cgB = false;
   }
 
   // symmetry-breaking upper bound (unlabeled only, src/gpu_match.cu:426-458)
@@ -257,7 +284,7 @@ __device__ int run_slot(const MatchArgs& a, const DPlan& P, WarpState& S, int32_
       else if (ub < v) ub = v;
     }
     if (ub == -1) ub = INT_MAX;
-    if (ub != INT_MAX) lenA = warp_lower_bound<PAGED>(A, lenA, (int)ub);
+    if (ub != INT_MAX) lenA = warp_lower_bound<PAGED>(A, lenA, (int)ub, cgA);
   }
 
   const int T = a.T;
@@ -275,9 +302,9 @@ __device__ int run_slot(const MatchArgs& a, const DPlan& P, WarpState& S, int32_
   for (int base = 0; base < scan; base += 32) {
     const int i = base + lane;
     const bool valid = i < scan;
-    const int x = valid ? ld<PAGED>(A + i) : 0;
+    const int x = valid ? ld<PAGED>(A + i, cgA) : 0;
     bool keep = valid;
-    if (kind == SLOT_INTERSECT && keep) keep = bsearch_in<PAGED>(B, lenB, x);
+    if (kind == SLOT_INTERSECT && keep) keep = bsearch_in<PAGED>(B, lenB, x, cgB);
     if (LABELED) {
       if (keep && !by_label) keep = (mask >> a.labels[x]) & 1u;
     } else if (kind == SLOT_COPY) {
@@ -300,8 +327,9 @@ __device__ int run_slot(const MatchArgs& a, const DPlan& P, WarpState& S, int32_
   }
   if (T && cnt > T) cnt = T;
   const int alenA = by_label ? full_len : lenA;
+  const int alenB = full_lenB >= 0 ? full_lenB : lenB;
   w.setops++;
-  w.bytes += 4ull * (unsigned long long)(alenA + lenB + cnt) + (LABELED ? (unsigned long long)alenA : 0ull);
+  w.bytes += 4ull * (unsigned long long)(alenA + alenB + cnt) + (LABELED ? (unsigned long long)alenA : 0ull);
   return cnt;
 }
 
@@ -339,7 +367,7 @@ __device__ void alias_slot(const MatchArgs& a, const DPlan& P, WarpState& S, int
     if (ub != INT_MAX) {
       if (PAGED) {
         ListRef r = adj<PAGED>(a, S, v, arena + a.slot_words, w);
-        lenA = warp_lower_bound<PAGED>(r.p, r.len, ub);
+        lenA = warp_lower_bound<PAGED>(r.p, r.len, ub, r.cg);
         __syncwarp();
         unpin(a.pg, r);
       } else {
@@ -355,7 +383,7 @@ __device__ void alias_slot(const MatchArgs& a, const DPlan& P, WarpState& S, int
     if (ub != INT_MAX) {
       if (PAGED) {
         ListRef r = adj<PAGED>(a, S, v, arena + a.slot_words, w);
-        lenA = warp_lower_bound<PAGED>(r.p, r.len, ub);
+        lenA = warp_lower_bound<PAGED>(r.p, r.len, ub, r.cg);
         __syncwarp();
         unpin(a.pg, r);
       } else {
@@ -395,11 +423,11 @@ __device__ __forceinline__ int run_level(const MatchArgs& a, const DPlan& P, War
 
 // First index of sorted A[0,len) whose element is >= x (one lane).
 template <bool CG = false>
-__device__ __forceinline__ int lane_lower_bound(const int32_t* A, int len, int x) {
+__device__ __forceinline__ int lane_lower_bound(const int32_t* A, int len, int x, bool cg = true) {
   int lo = 0, hi = len;
   while (lo < hi) {
     const int mid = (lo + hi) >> 1;
-    if (ld<CG>(A + mid) < x) lo = mid + 1; else hi = mid;
+    if (ld<CG>(A + mid, cg) < x) lo = mid + 1; else hi = mid;
   }
   return lo;
 }
@@ -412,13 +440,13 @@ __device__ __forceinline__ int lane_lower_bound(const int32_t* A, int len, int x
 // (the caller hands the candidate to the whole warp).
 template <bool LABELED, bool CG>
 __device__ __forceinline__ int lane_intersect(const int32_t* A, int deg, int ub, const int32_t* B, int lenB,
-                                              const uint8_t* labels, uint32_t mask, int* lenA) {
+                                              const uint8_t* labels, uint32_t mask, int* lenA, bool cg) {
   int k = 0, p = 0, x = 0;
   while (true) {
     if (x >= PM_LANE_MAX) return -1;
     int v[4];
 #pragma unroll
-    for (int q = 0; q < 4; q++) v[q] = (x + q < deg) ? ld<CG>(A + x + q) : INT_MAX;
+    for (int q = 0; q < 4; q++) v[q] = (x + q < deg) ? ld<CG>(A + x + q, cg) : INT_MAX;
 #pragma unroll
     for (int q = 0; q < 4; q++) {
       const int val = v[q];
@@ -434,7 +462,7 @@ __device__ __forceinline__ int lane_intersect(const int32_t* A, int deg, int ub,
       if (p < lenB && B[p] == val && (!LABELED || ((mask >> labels[val]) & 1u))) k++;
       if (p >= lenB) {  // the rest of A is above all of B: only its length matters
         const int r0 = x + q + 1;
-        *lenA = r0 + lane_lower_bound<CG>(A + r0, deg - r0, ub);
+        *lenA = r0 + lane_lower_bound<CG>(A + r0, deg - r0, ub, cg);
         return k;
       }
     }
@@ -511,34 +539,42 @@ __device__ unsigned long long leaf_batch(const MatchArgs& a, const DPlan& P, War
       } else {
         const uint64_t rb = a.rowptr[c];
         const int deg = (int)(a.rowptr[c + 1] - rb);
-        const int32_t* A = PAGED ? nullptr : a.colidx + rb;
+        // a one-label mask reads only that label's part of the list
+        const bool grouped = LABELED && a.lab_off && __popc(mask) == 1;
+        const int2 gr = grouped ? label_range(a, c, __ffs(mask) - 1) : make_int2(0, deg);
+        const int32_t* A = PAGED ? nullptr : (grouped ? a.colidx_lab + rb + gr.x : a.colidx + rb);
         int32_t pinned = -1;
+        bool cgl = false;  // A sits in an evictable frame
         if (PAGED) {
-          // this lane's own list when its one page is resident (pinned and
-          // read from the frame); a missing page or a list over several pages
-          // goes to the warp, which reads host memory coalesced, gathers and
-          // requests the page
+          // this lane's own list (or label part) when its one page is
+          // resident (pinned and read from the frame) or it spans consecutive
+          // static frames; a missing page, a list over evictable pages, or a
+          // whole sorted list of a labeled graph (host memory) goes to the
+          // warp, which reads host memory coalesced, gathers and requests pages
+          const uint64_t s0 = rb + (uint64_t)gr.x;
           const int sh = a.pg.page_shift;
-          const int32_t p0 = (int32_t)(rb >> sh);
-          const int32_t p1 = deg ? (int32_t)((rb + (uint64_t)deg - 1) >> sh) : p0;
-          if (deg == 0) {
-            A = a.pg.host_colidx + rb;  // nothing is read
+          if (LABELED && !grouped) {
+            deferred = true;
+          } else if (gr.y == 0) {
+            A = a.pg.host_colidx + s0;  // nothing is read
           } else {
+            const int32_t p0 = (int32_t)(s0 >> sh);
+            const int32_t p1 = (int32_t)((s0 + (uint64_t)gr.y - 1) >> sh);
             const int32_t f = (p0 == p1) ? (pinned = try_pin(a.pg, p0)) : static_run(a.pg, p0, p1);
             if (f < 0) {
               deferred = true;
             } else {
-              A = a.pg.frames + ((uint64_t)f << sh) + (rb & ((1ull << sh) - 1));
+              A = a.pg.frames + ((uint64_t)f << sh) + (s0 & ((1ull << sh) - 1));
+              cgl = f >= a.pg.n_static;
               lpc_hits++;
             }
           }
         }
-        const bool grouped = LABELED && !PAGED && a.colidx_lab && __popc(mask) == 1;
         if (deferred) {
           // handled by the warp below
         } else if (kind == SLOT_INTERSECT && !grouped) {
           int lenA = 0;
-          int k = lane_intersect<LABELED, PAGED>(A, deg, ub, Bs, lenB, a.labels, mask, &lenA);
+          int k = lane_intersect<LABELED, PAGED>(A, deg, ub, Bs, lenB, a.labels, mask, &lenA, cgl);
           if (k < 0) {
             deferred = true;
           } else {
@@ -548,15 +584,12 @@ __device__ unsigned long long leaf_batch(const MatchArgs& a, const DPlan& P, War
             ops++;
           }
         } else {
-        const int lenA = (ub == INT_MAX) ? deg : lane_lower_bound<PAGED>(A, deg, ub);
+        const int lenA = (ub == INT_MAX) ? deg : lane_lower_bound<PAGED>(A, deg, ub, cgl);
         if (grouped) {
           // the label-l part of the list: a fresh set is its length, an
           // intersection merges only it
-          const int32_t* o = a.lab_off + (int64_t)c * a.nl1;
-          const int l = __ffs(mask) - 1;
-          const bool present = l < a.nl1 - 1;  // a label no vertex carries: empty
-          const int32_t* Al = a.colidx_lab + rb + (present ? o[l] : 0);
-          const int lenl = present ? o[l + 1] - o[l] : 0;
+          const int32_t* Al = A;
+          const int lenl = gr.y;
           int k = 0;
           if (kind == SLOT_FRESH) {
             k = lenl;
@@ -565,7 +598,7 @@ __device__ unsigned long long leaf_batch(const MatchArgs& a, const DPlan& P, War
           } else {
             int p = 0;
             for (int x = 0; x < lenl && p < lenB; x++) {
-              const int v = Al[x];
+              const int v = ld<PAGED>(Al + x, cgl);
               int lo = p, step = 1;
               while (lo + step < lenB && Bs[lo + step] < v) { lo += step; step <<= 1; }
               int hi = min(lo + step + 1, lenB);
@@ -590,8 +623,8 @@ __device__ unsigned long long leaf_batch(const MatchArgs& a, const DPlan& P, War
           int k = lim;
           for (int j = 0; j <= L; j++) {
             const int pj = S.path[j];
-            const int pos = lane_lower_bound<PAGED>(A, lim, pj);
-            k -= (pos < lim && ld<PAGED>(A + pos) == pj) ? 1 : 0;
+            const int pos = lane_lower_bound<PAGED>(A, lim, pj, cgl);
+            k -= (pos < lim && ld<PAGED>(A + pos, cgl) == pj) ? 1 : 0;
           }
           cnt += k;
           bytes += 4ull * (unsigned long long)(lenA + k);
@@ -600,7 +633,7 @@ __device__ unsigned long long leaf_batch(const MatchArgs& a, const DPlan& P, War
           deferred = true;
         } else if (kind == SLOT_FRESH) {  // labeled: label filter only
           int k = 0;
-          for (int x = 0; x < lenA; x++) k += (mask >> a.labels[ld<PAGED>(A + x)]) & 1u;
+          for (int x = 0; x < lenA; x++) k += (mask >> a.labels[ld<PAGED>(A + x, cgl)]) & 1u;
           if (T && k > T) k = T;
           cnt += k;
           bytes += 4ull * (unsigned long long)(lenA + k) + (unsigned long long)lenA;
@@ -608,7 +641,7 @@ __device__ unsigned long long leaf_batch(const MatchArgs& a, const DPlan& P, War
         } else {  // intersection with the common operand
           int k = 0, p = 0;
           for (int x = 0; x < lenA && p < lenB; x++) {
-            const int v = ld<PAGED>(A + x);
+            const int v = ld<PAGED>(A + x, cgl);
             int lo = p, step = 1;
             while (lo + step < lenB && Bs[lo + step] < v) { lo += step; step <<= 1; }
             int hi = min(lo + step + 1, lenB);
@@ -662,8 +695,10 @@ struct Donation {
 
 // Hands the upper half of the shallowest level range that is long enough to
 // the donation ring, when some warps are idle and fewer pieces are queued
-// than idle warps.  Lane 0 decides.
-__device__ __forceinline__ void maybe_donate(const MatchArgs& a, WarpState& S, int L0, int L, int plan_id,
+// than idle warps.  A range whose candidates head whole subtrees is long
+// enough from 2 candidates on; one whose candidates only lead to the last
+// level (one set operation each) needs split_min.  Lane 0 decides.
+__device__ __forceinline__ void maybe_donate(const MatchArgs& a, WarpState& S, int n, int L0, int L, int plan_id,
                                              int root_id) {
   const int lane = lane_id();
   if (lane == 0) {
@@ -674,7 +709,7 @@ __device__ __forceinline__ void maybe_donate(const MatchArgs& a, WarpState& S, i
         head - tail < (unsigned long long)a.don_mask) {
       for (int k = L0; k <= L; k++) {
         const int it = S.iter[k], iend = S.iend[k];
-        if (iend - it < max(a.split_min, 2)) continue;
+        if (iend - it < ((k + 1 == n - 2) ? max(a.split_min, 2) : 2)) continue;
         const int mid = it + (iend - it) / 2;  // it < mid < iend
         const unsigned long long slot = atomicAdd(a.don_head, 1ull);
         int4* dst = a.don_items + 3 * (slot & a.don_mask);
@@ -737,7 +772,7 @@ __device__ unsigned long long dfs_from(const MatchArgs& a, const DPlan& P, WarpS
     }
     if (a.split_min > 0 && w.setops >= S.next_split) {
       if (lane == 0) S.next_split = w.setops + 64;
-      maybe_donate(a, S, L0, L, plan_id, root_id);
+      maybe_donate(a, S, n, L0, L, plan_id, root_id);
     }
     const int m = P.level_begin[L];
     const int it = S.iter[L];
@@ -976,15 +1011,17 @@ __global__ void maxnbrdeg_kernel(const uint64_t* rowptr, const int32_t* colidx, 
 }
 
 // Regroups each list by label, keeping id order within a label (a stable
-// partition): one warp per vertex, ranks from __match_any_sync.
-__global__ void label_group_kernel(const uint64_t* rowptr, const int32_t* colidx, const uint8_t* labels, int64_t n,
-                                   int nl1, int32_t* out, int32_t* off) {
+// partition): one warp per vertex, ranks from __match_any_sync.  Vertices
+// [v_begin, v_end); entry i of the adjacency array lands at out[i - out_base].
+__global__ void label_group_kernel(const uint64_t* rowptr, const int32_t* colidx, const uint8_t* labels,
+                                   int64_t v_begin, int64_t v_end, int nl1, int32_t* out, uint64_t out_base,
+                                   int32_t* off) {
   __shared__ int base_s[16][33];
   const int lane = lane_id();
   const int wib = threadIdx.x >> 5;
   int* base = base_s[wib];
   const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
-  for (long long v = (long long)blockIdx.x * (blockDim.x >> 5) + wib; v < n; v += warps) {
+  for (long long v = v_begin + (long long)blockIdx.x * (blockDim.x >> 5) + wib; v < v_end; v += warps) {
     const uint64_t b = rowptr[v], e = rowptr[v + 1];
     // per-label counts: lane l counts label l
     int mine = 0;
@@ -1015,7 +1052,7 @@ __global__ void label_group_kernel(const uint64_t* rowptr, const int32_t* colidx
       const int x = valid ? colidx[i] : 0;
       const int lb = valid ? (int)labels[x] : 32 + lane;  // invalid lanes match only themselves
       const unsigned same = __match_any_sync(FULL, lb);
-      if (valid) out[b + base[lb] + __popc(same & lanemask_lt())] = x;
+      if (valid) out[b - out_base + base[lb] + __popc(same & lanemask_lt())] = x;
       __syncwarp();
       if (valid && (same & lanemask_lt()) == 0) base[lb] += __popc(same);
       __syncwarp();
@@ -1184,11 +1221,45 @@ static pm_status graph_finish(pm_graph* g) {
     CK(cudaMalloc(&g->d_lab_off, sizeof(int32_t) * (size_t)g->n * g->nl1));
     g->device_bytes += sizeof(int32_t) * ((size_t)g->nadj + (size_t)g->n * g->nl1);
     (void)cudaGetLastError();  // drop a stale error from an earlier call
-    label_group_kernel<<<2048, 256>>>(g->d_rowptr, g->d_colidx, g->d_labels, g->n, g->nl1, g->d_colidx_lab,
+    label_group_kernel<<<2048, 256>>>(g->d_rowptr, g->d_colidx, g->d_labels, 0, g->n, g->nl1, g->d_colidx_lab, 0,
                                       g->d_lab_off);
     CK(cudaGetLastError());
     CK(cudaDeviceSynchronize());
   }
+  return PM_OK;
+}
+
+// Labeled paged graphs: the label-grouped copy of the adjacency array goes to
+// pinned host memory (it is what the frames cache), the group offsets to the
+// device.  Grouped on the device from the host array, a vertex range at a
+// time through a bounded device buffer.
+static pm_status paged_group_labels(pm_graph* g, const uint64_t* h_rowptr) {
+  g->nl1 = (g->nlabels > 0 ? g->nlabels : 32) + 1;
+  CK(cudaHostAlloc((void**)&g->h_colidx_lab, sizeof(int32_t) * std::max<int64_t>(g->nadj, 1),
+                   cudaHostAllocMapped | cudaHostAllocPortable));
+  CK(cudaHostGetDevicePointer((void**)&g->h_colidx_lab_dev, g->h_colidx_lab, 0));
+  CK(cudaMalloc(&g->d_lab_off, sizeof(int32_t) * (size_t)std::max<int64_t>(g->n, 1) * g->nl1));
+  g->device_bytes += sizeof(int32_t) * (size_t)g->n * g->nl1;
+  const int64_t chunk = std::max<int64_t>(g->maxdeg, std::min<int64_t>(std::max<int64_t>(g->nadj, 1), 64ll << 20));
+  int32_t* tmp = nullptr;
+  CK(cudaMalloc(&tmp, sizeof(int32_t) * (size_t)std::max<int64_t>(chunk, 1)));
+  pm_status st = PM_OK;
+  for (int64_t v0 = 0; v0 < g->n && st == PM_OK;) {
+    int64_t v1 = v0;
+    while (v1 < g->n && (int64_t)(h_rowptr[v1 + 1] - h_rowptr[v0]) <= chunk) v1++;
+    const uint64_t b0 = h_rowptr[v0], len = h_rowptr[v1] - b0;
+    (void)cudaGetLastError();  // drop a stale error from an earlier call
+    label_group_kernel<<<2048, 256>>>(g->d_rowptr, g->h_colidx_dev, g->d_labels, v0, v1, g->nl1, tmp, b0,
+                                      g->d_lab_off);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess && len) e = cudaMemcpy(g->h_colidx_lab + b0, tmp, sizeof(int32_t) * len, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) st = fail(PM_ERR_CUDA, "label grouping: %s", cudaGetErrorString(e));
+    v0 = v1;
+  }
+  cudaFree(tmp);
+  if (st != PM_OK) return st;
+  g->h_paged = g->h_colidx_lab;
+  g->h_paged_dev = g->h_colidx_lab_dev;
   return PM_OK;
 }
 
@@ -1254,6 +1325,10 @@ extern "C" pm_status pm_graph_from_host(int64_t n, int64_t nadj, const uint64_t*
     g->device_bytes += sizeof(int32_t) * g->n;
     st = paged_maxnbrdeg(g.get());
     if (st != PM_OK) return st;
+    if (g->labeled && n > 0) {
+      st = paged_group_labels(g.get(), rowptr);
+      if (st != PM_OK) return st;
+    }
   } else {
     CK(cudaMalloc(&g->d_colidx, sizeof(int32_t) * std::max<int64_t>(nadj, 1)));
     if (nadj) CK(cudaMemcpy(g->d_colidx, colidx, sizeof(int32_t) * nadj, cudaMemcpyHostToDevice));
@@ -1587,6 +1662,7 @@ static pm_status setup_launch(pm_ctx* c, const pm_graph* g, const pm_plan* const
   a.labels = g->d_labels;
   a.colidx_lab = g->d_colidx_lab;
   a.lab_off = g->d_lab_off;
+  a.host_sorted = (g->residency == PM_RESIDENT_PAGED && g->d_lab_off) ? g->h_colidx_dev : nullptr;
   a.nl1 = g->nl1;
   a.n = (int32_t)g->n;
   a.nplans = nplans;

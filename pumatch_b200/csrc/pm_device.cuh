@@ -50,7 +50,7 @@ struct DPaging {
   int32_t* frame_pin;              // [n_frames]: readers in flight
   uint8_t* frame_ref;              // [n_frames]: CLOCK reference bits
   int32_t* frames;                 // [n_frames << page_shift]
-  const int32_t* host_colidx;      // device-visible pointer to pinned host colidx
+  const int32_t* host_colidx;      // device-visible pointer to the paged host array
   unsigned long long* clock_hand;  // device
   unsigned long long* next_free;   // device: frames handed out so far
   unsigned long long* ring_head;   // device: ring slots reserved
@@ -90,6 +90,12 @@ struct pm_graph {
   // paged residency (pm_paging.cu)
   int32_t* h_colidx = nullptr;     // pinned, mapped copy of the adjacency array
   int32_t* h_colidx_dev = nullptr; // its device-visible address
+  // labeled paged graphs page the label-grouped copy (d_lab_off on the
+  // device gives the groups); unlabeled ones page colidx itself
+  int32_t* h_colidx_lab = nullptr;     // pinned, mapped
+  int32_t* h_colidx_lab_dev = nullptr;
+  const int32_t* h_paged = nullptr;    // host array the pages are cut from
+  const int32_t* h_paged_dev = nullptr;
   uint32_t page_ints = 0;
   int64_t n_pages = 0, n_frames = 0;
   pm::PagedState* ps = nullptr;

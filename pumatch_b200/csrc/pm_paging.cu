@@ -108,7 +108,7 @@ static pm_status reset_table(pm_graph* g, cudaStream_t st, bool cold) {
     while (e < pre && e != s->n_static && fp[e] == fp[e - 1] + 1) e++;
     const int64_t first = (int64_t)fp[f] * g->page_ints;
     const size_t bytes = std::min<size_t>((size_t)(e - f) * pb, sizeof(int32_t) * (size_t)(g->nadj - first));
-    CKP(cudaMemcpyAsync((char*)s->frames + (size_t)f * pb, g->h_colidx + first, bytes, cudaMemcpyHostToDevice, st));
+    CKP(cudaMemcpyAsync((char*)s->frames + (size_t)f * pb, g->h_paged + first, bytes, cudaMemcpyHostToDevice, st));
     f = e;
   }
   CKP(cudaMemsetAsync(s->frame_pin, 0, sizeof(int32_t) * g->n_frames, st));
@@ -174,6 +174,8 @@ pm_status paged_place(pm_graph* g, const int32_t* colidx, const pm_graph_opts* o
     }
   }
   CKP(cudaHostGetDevicePointer((void**)&g->h_colidx_dev, g->h_colidx, 0));
+  g->h_paged = g->h_colidx;  // a labeled graph switches to its label-grouped copy after placement
+  g->h_paged_dev = g->h_colidx_dev;
   // device page table and frame pool
   const size_t fbytes = (size_t)g->n_frames * pb;
   CKP(cudaMalloc(&s->frames, std::max<size_t>(fbytes, 4)));
@@ -206,9 +208,9 @@ pm_status paged_place(pm_graph* g, const int32_t* colidx, const pm_graph_opts* o
   g->ps = s.release();
   std::vector<int64_t> prefix((size_t)g->n_frames);
   for (int64_t f = 0; f < g->n_frames; f++) prefix[f] = f;
-  pm_status st = set_initial(g, std::move(prefix));
-  if (st != PM_OK) return st;
-  return reset_table(g, g->ps->copy_stream, false);
+  // the frames are filled by the first run (static_loaded is false), after a
+  // labeled graph has switched to its grouped copy
+  return set_initial(g, std::move(prefix));
 }
 
 int64_t paged_static_frames(const pm_graph* g) { return g->ps ? g->ps->n_static : 0; }
@@ -225,7 +227,9 @@ void paged_release(pm_graph* g) {
     g->ps = nullptr;
   }
   if (g->h_colidx) cudaFreeHost(g->h_colidx);
-  g->h_colidx = nullptr;
+  if (g->h_colidx_lab) cudaFreeHost(g->h_colidx_lab);
+  g->h_colidx = g->h_colidx_lab = nullptr;
+  g->h_paged = nullptr;
 }
 
 pm_status paged_prepare(pm_ctx* c, pm_graph* g, bool cold, DPaging* out) {
@@ -246,7 +250,7 @@ pm_status paged_prepare(pm_ctx* c, pm_graph* g, bool cold, DPaging* out) {
   out->frame_pin = s->frame_pin;
   out->frame_ref = s->frame_ref;
   out->frames = s->frames;
-  out->host_colidx = g->h_colidx_dev;
+  out->host_colidx = g->h_paged_dev;
   out->clock_hand = s->dctl;
   out->next_free = s->dctl + 1;
   out->ring_head = s->dctl + 2;
@@ -275,7 +279,7 @@ static void service_loop(pm_graph* g) {
       if (req.x < 0) { s->noops++; continue; }
       const int64_t first = (int64_t)req.x * g->page_ints;
       const size_t bytes = std::min<size_t>(pb, sizeof(int32_t) * (size_t)(nadj - first));
-      cudaError_t e = cudaMemcpyAsync((char*)s->frames + (size_t)req.y * pb, g->h_colidx + first, bytes,
+      cudaError_t e = cudaMemcpyAsync((char*)s->frames + (size_t)req.y * pb, g->h_paged + first, bytes,
                                       cudaMemcpyHostToDevice, s->copy_stream);
       if (e == cudaSuccess)
         e = cudaMemcpyAsync(s->page_frame + req.x, s->stage + req.y, sizeof(int32_t), cudaMemcpyHostToDevice,

@@ -133,6 +133,7 @@ struct ListRef {
   const int32_t* p;
   int len;
   int32_t pinned;  // frame to unpin after use, or -1
+  bool cg;         // an evictable frame: read through L2 only (refilled during the launch)
 };
 
 // Most pages one list may span and still be gathered from frames; longer
@@ -182,7 +183,7 @@ static __device__ ListRef paged_list(const DPaging& pg, uint64_t b, int len, int
   f0 = __shfl_sync(0xffffffffu, f0, 0);
   if (mode == 0) {
     const uint64_t off = b & ((1ull << sh) - 1);
-    return ListRef{pg.frames + ((uint64_t)f0 << sh) + off, len, f0};
+    return ListRef{pg.frames + ((uint64_t)f0 << sh) + off, len, f0, f0 >= pg.n_static};
   }
   if (mode == 1) return ListRef{pg.host_colidx + b, len, -1};
   // gather the pinned pages into the arena, then unpin them
