@@ -47,24 +47,25 @@ WORKLOADS = {
     # the same graph with 16 uniform labels and the 7-cycle (labeled semantics)
     "chunglu100k_c7_lab16": dict(graph=_CL100K, labeled=True, n_labels=16, label_seed=102, pattern_label_seed=202,
                                  patterns=[("C7", P.cycle(7))]),
-    # the K7 query with the adjacency in host memory: half of it in static
-    # frames (the reference's device partition holds the first 60% of the
-    # edges) plus an evictable tenth
+    # the K7 query with the adjacency in host memory: 60% of it in static
+    # frames (the reference's device partition: the first 60% of the edges)
+    # plus evictable frames for 28% (its 4 GB package buffer against the
+    # 14.4 GB adjacency of the configured R-MAT graph)
     "chunglu100k_k7_paged": dict(graph=_CL100K, labeled=False, n_labels=0, patterns=[("K7", P.clique(7))],
-                                 paged=dict(frame_fraction=0.6, static_fraction=0.5, page_bytes=16 << 10)),
+                                 paged=dict(frame_fraction=0.88, static_fraction=0.6, page_bytes=16 << 10)),
     # R-MAT (a,b,c = .57,.19,.19) 1M vertices / 16M edges, 32 labels, the
     # 5-cycle plus 2-vertex pendant path, in HBM and paged (the same pool split)
     "rmat1m_c5t2_lab32": dict(graph=_RMAT1M, labeled=True, n_labels=32, label_seed=102, pattern_label_seed=202,
                               patterns=[("C5t2", P.cycle_tail(5, 2))]),
     "rmat1m_c5t2_lab32_paged": dict(graph=_RMAT1M, labeled=True, n_labels=32, label_seed=102,
                                     pattern_label_seed=202, patterns=[("C5t2", P.cycle_tail(5, 2))],
-                                    paged=dict(frame_fraction=0.6, static_fraction=0.5, page_bytes=64 << 10)),
+                                    paged=dict(frame_fraction=0.88, static_fraction=0.6, page_bytes=64 << 10)),
     # twenty seeded 4-7-vertex patterns in one persistent launch
     "rmat128k_batch20_lab32": dict(graph=_RMAT128K, labeled=True, n_labels=32, label_seed=102, batch_seed=303),
     # learned-scheduler comparison (--learned): trained on seeds 11, 12, 13
     "rmat128k_c5t2_lab32_paged": dict(graph=_RMAT128K, labeled=True, n_labels=32, label_seed=102,
                                       pattern_label_seed=202, patterns=[("C5t2", P.cycle_tail(5, 2))],
-                                      paged=dict(frame_fraction=0.3, static_fraction=0.25, page_bytes=16 << 10)),
+                                      paged=dict(frame_fraction=0.88, static_fraction=0.6, page_bytes=16 << 10)),
 }
 DEFAULT_WORKLOAD = "chunglu100k_k7"
 
@@ -263,7 +264,8 @@ def run_ours(args, workload):
     stream = torch.cuda.ExternalStream(ctx.stream_ptr, device=torch.device("cuda", local))
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")  # > 126 MB L2
     shard = dict(shard_rank=rank, shard_count=world) if world > 1 else {}
-    run_kw = dict(timeout_ms=args.timeout_s * 1000, high_occupancy=args.high_occupancy, **shard)
+    run_kw = dict(timeout_ms=args.timeout_s * 1000, high_occupancy=args.high_occupancy,
+                  leaf_per_lane=int(args.leaf_per_lane), **shard)
     if args.root_limit > 0:
         run_kw.update(root_begin=args.root_begin, root_end=args.root_begin + args.root_limit)
 
@@ -350,7 +352,8 @@ def run_ours(args, workload):
             "data": "synthetic",
             "config": {"workload": workload, "graph": w["graph"], "labeled": w["labeled"],
                        "patterns": [p for p, _ in texts], "counts": counts_total,
-                       "kernel_variant": ["default", "regs64", "regs85"][args.high_occupancy],
+                       "kernel_variant": ["default", "regs64", "regs85"][args.high_occupancy] +
+                                         ("+leaf_per_lane" if args.leaf_per_lane else ""),
                        "root_limit": args.root_limit or None,
                        "roots": int(st["n_roots"]), "set_ops_per_step": set_ops // args.steps,
                        "donated_ranges_last_step": int(st["splits"]),
@@ -519,6 +522,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--high-occupancy", type=int, default=0,
                     help="kernel variant: 0 no register cap, 1 capped at 64, 2 capped at 85")
+    ap.add_argument("--leaf-per-lane", action="store_true",
+                    help="last level one candidate per lane instead of work-balanced across the warp")
     ap.add_argument("--root-limit", type=int, default=0, help="profile this many roots only (from --root-begin)")
     ap.add_argument("--root-begin", type=int, default=0)
     ap.add_argument("--learned", action="store_true", help="plain vs learned scheduling on the workload")

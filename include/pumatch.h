@@ -226,7 +226,11 @@ typedef struct {
                                spills (default); 1 capped at 64 registers
                                (four 256-thread blocks per SM); 2 capped at
                                85 (three blocks per SM)                      */
-  int32_t reserved_[2];
+  int32_t leaf_per_lane;    /* 1: last-level intersections one candidate per
+                               lane (long lists go to the warp); 0 (default):
+                               work-balanced across the warp when the common
+                               operand fits in shared memory                 */
+  int32_t reserved_;
   uint64_t* root_counts;    /* optional device ptr: per-root counts (plan 0) */
   float* root_cost;         /* optional device ptr: per-root set-op bytes    */
   const int32_t* root_order;/* optional device ptr: process roots in this

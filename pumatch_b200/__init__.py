@@ -63,7 +63,7 @@ class RunOpts(C.Structure):
                 ("chunk", C.c_int32), ("split_level1", C.c_int32), ("shard_rank", C.c_int32),
                 ("shard_count", C.c_int32), ("use_graph", C.c_int32), ("timeout_ms", C.c_int32),
                 ("root_begin", C.c_int64), ("root_end", C.c_int64), ("cold_cache", C.c_int32),
-                ("high_occupancy", C.c_int32), ("reserved_", C.c_int32 * 2),
+                ("high_occupancy", C.c_int32), ("leaf_per_lane", C.c_int32), ("reserved_", C.c_int32),
                 ("root_counts", C.c_void_p), ("root_cost", C.c_void_p), ("root_order", C.c_void_p),
                 ("root_reads", C.c_void_p)]
 

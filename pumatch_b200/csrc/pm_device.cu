@@ -76,6 +76,8 @@ struct MatchArgs {
   const int32_t* colidx_lab;    // label-grouped lists (labeled, HBM) or null
   const int32_t* lab_off;       // label group offsets (labeled, HBM or paged) or null
   const int32_t* host_sorted;   // labeled paged: the id-sorted lists in mapped host memory
+  int32_t leaf_flat;            // last-level intersections work-balanced across the warp (leaf_flat)
+  int32_t pad2;
   int32_t nl1;
   int32_t pad1;
   int32_t n;
@@ -470,6 +472,98 @@ __device__ __forceinline__ int lane_intersect(const int32_t* A, int deg, int ub,
   }
 }
 
+// Membership of x (>= 0) in an open-addressing table of 2^bits slots, empty
+// slots -1, at most half full (so every probe run ends at an empty slot).
+__device__ __forceinline__ bool in_table(const int32_t* t, int bits, int x) {
+  unsigned h = ((unsigned)x * 0x9E3779B1u) >> (32 - bits);
+  const unsigned m = (1u << bits) - 1;
+  while (true) {
+    const int y = t[h];
+    if (y == x) return true;
+    if (y < 0) return false;
+    h = (h + 1) & m;
+  }
+}
+
+// The last-level intersections of candidates [b, e) with the common operand B
+// (|B| <= PM_SB_MAX), work-balanced across the warp: the first operands of 32
+// candidates (each cut at its symmetry-breaking bound) are laid end to end
+// and every lane takes every 32nd element, finds its owner by a binary
+// search over the lanes' offsets, and tests it against B in shared memory
+// (a hash table when |B| <= PM_SB_MAX / 2, else the sorted copy).  Counts
+// only; no truncation.  Same set operations, counts and accounting as
+// lane_intersect per candidate.
+template <bool LABELED>
+__device__ unsigned long long leaf_flat(const MatchArgs& a, WarpState& S, const int32_t* cand, int b, int e,
+                                        const int32_t* B, int lenB, uint32_t mask, int common_ub, bool self_ub,
+                                        Work& w) {
+  const int lane = lane_id();
+  const bool hashed = lenB <= PM_SB_MAX / 2;
+  int bits = 5;
+  if (hashed) {
+    while ((1 << bits) < 2 * lenB) bits++;  // 2^bits <= PM_SB_MAX
+    const int size = 1 << bits;
+    for (int i = lane; i < size; i += 32) S.sb[i] = -1;
+    __syncwarp();
+    for (int i = lane; i < lenB; i += 32) {
+      const int x = B[i];
+      unsigned h = ((unsigned)x * 0x9E3779B1u) >> (32 - bits);
+      while (atomicCAS(&S.sb[h], -1, x) != -1) h = (h + 1) & (unsigned)(size - 1);
+    }
+  } else {
+    for (int i = lane; i < lenB; i += 32) S.sb[i] = B[i];
+  }
+  __syncwarp();
+  unsigned long long cnt = 0, bytes = 0, ops = 0;  // per lane
+  for (int base = b; base < e; base += 32) {
+    const int i = base + lane;
+    const bool mine = i < e;
+    int lenA = 0;
+    unsigned long long rb = 0;
+    if (mine) {
+      const int c = cand[i];
+      rb = a.rowptr[c];
+      const int deg = (int)(a.rowptr[c + 1] - rb);
+      const int ub = self_ub ? min(common_ub, c) : common_ub;
+      lenA = (ub == INT_MAX) ? deg : lane_lower_bound(a.colidx + rb, deg, ub);
+      bytes += 4ull * (unsigned long long)(lenA + lenB) + (LABELED ? (unsigned long long)lenA : 0ull);
+      ops++;
+    }
+    int incl = lenA;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(FULL, incl, o);
+      if (lane >= o) incl += t;
+    }
+    const int excl = incl - lenA;
+    const int total = __shfl_sync(FULL, incl, 31);
+    for (int t0 = 0; t0 < total; t0 += 32) {
+      const int t = t0 + lane;
+      int j = 0, ej = 0;  // the last lane whose offset is <= t owns element t
+#pragma unroll
+      for (int step = 16; step; step >>= 1) {
+        const int e2 = __shfl_sync(FULL, excl, j + step);
+        if (e2 <= t) { j += step; ej = e2; }
+      }
+      const unsigned long long rbj = __shfl_sync(FULL, rb, j);
+      if (t < total) {
+        const int x = a.colidx[rbj + (unsigned long long)(t - ej)];
+        bool hit = hashed ? in_table(S.sb, bits, x) : bsearch_in<false>(S.sb, lenB, x);
+        if (LABELED && hit) hit = (mask >> a.labels[x]) & 1u;
+        cnt += hit ? 1u : 0u;
+      }
+    }
+  }
+  bytes += 4ull * cnt;  // the results
+  for (int o = 16; o; o >>= 1) {
+    cnt += __shfl_xor_sync(FULL, cnt, o);
+    bytes += __shfl_xor_sync(FULL, bytes, o);
+    ops += __shfl_xor_sync(FULL, ops, o);
+  }
+  w.setops += ops;
+  w.bytes += bytes;
+  return cnt;
+}
+
 // The last level for the candidates [b, e) of level L's main slot (each is
 // v_{n-2} in turn): one lane per candidate, counting only.  Same set
 // operations and counts as run_slot(last) per candidate, organised so that
@@ -513,6 +607,9 @@ __device__ unsigned long long leaf_batch(const MatchArgs& a, const DPlan& P, War
       if (P.partial[s] & (1u << j)) common_ub = min(common_ub, S.path[j]);
     self_ub = (P.partial[s] >> Lf) & 1u;
   }
+  if (!PAGED && kind == SLOT_INTERSECT && T == 0 && lenB <= PM_SB_MAX && a.leaf_flat &&
+      !(LABELED && a.lab_off && __popc(mask) == 1))
+    return leaf_flat<LABELED>(a, S, cand, b, e, B, lenB, mask, common_ub, self_ub, w);
   const int32_t* Bs = B;
   if (kind == SLOT_INTERSECT && lenB <= PM_SB_MAX) {
     for (int i = lane; i < lenB; i += 32) S.sb[i] = B[i];
@@ -520,7 +617,7 @@ __device__ unsigned long long leaf_batch(const MatchArgs& a, const DPlan& P, War
     Bs = S.sb;
   }
   unsigned long long cnt = 0, bytes = 0, ops = 0;  // per lane
-  unsigned long long lpc_hits = 0;                 // per lane (paged residency)
+  PageCounters lpc = {};                           // per lane (paged residency)
   for (int base = b; base < e; base += 32) {
     const int i = base + lane;
     const bool mine = i < e;
@@ -561,12 +658,19 @@ __device__ unsigned long long leaf_batch(const MatchArgs& a, const DPlan& P, War
             const int32_t p0 = (int32_t)(s0 >> sh);
             const int32_t p1 = (int32_t)((s0 + (uint64_t)gr.y - 1) >> sh);
             const int32_t f = (p0 == p1) ? (pinned = try_pin(a.pg, p0)) : static_run(a.pg, p0, p1);
-            if (f < 0) {
-              deferred = true;
-            } else {
+            if (f >= 0) {
               A = a.pg.frames + ((uint64_t)f << sh) + (s0 & ((1ull << sh) - 1));
               cgl = f >= a.pg.n_static;
-              lpc_hits++;
+              lpc.hits++;
+            } else if (p0 == p1 && gr.y <= PM_LANE_MAX) {
+              // a short list on a missing page: this lane reads it from host
+              // memory (a warp keeps 32 such reads in flight) and asks for the page
+              if (ld_vol(&a.pg.page_frame[p0]) == PAGE_ABSENT) request_page(a.pg, p0, lpc);
+              A = a.pg.host_colidx + s0;
+              lpc.misses++;
+              lpc.zc_bytes += 4ull * (unsigned long long)gr.y;
+            } else {
+              deferred = true;
             }
           }
         }
@@ -673,8 +777,16 @@ __device__ unsigned long long leaf_batch(const MatchArgs& a, const DPlan& P, War
     }
   }
   if (PAGED) {
-    for (int o = 16; o; o >>= 1) lpc_hits += __shfl_xor_sync(FULL, lpc_hits, o);
-    w.pc.hits += lpc_hits;
+    unsigned long long v[6] = {lpc.hits, lpc.misses, lpc.zc_bytes, lpc.requests, lpc.evictions, lpc.dropped};
+#pragma unroll
+    for (int k = 0; k < 6; k++)
+      for (int o = 16; o; o >>= 1) v[k] += __shfl_xor_sync(FULL, v[k], o);
+    w.pc.hits += v[0];
+    w.pc.misses += v[1];
+    w.pc.zc_bytes += v[2];
+    w.pc.requests += v[3];
+    w.pc.evictions += v[4];
+    w.pc.dropped += v[5];
   }
   for (int o = 16; o; o >>= 1) {
     cnt += __shfl_xor_sync(FULL, cnt, o);
@@ -1663,6 +1775,7 @@ static pm_status setup_launch(pm_ctx* c, const pm_graph* g, const pm_plan* const
   a.colidx_lab = g->d_colidx_lab;
   a.lab_off = g->d_lab_off;
   a.host_sorted = (g->residency == PM_RESIDENT_PAGED && g->d_lab_off) ? g->h_colidx_dev : nullptr;
+  a.leaf_flat = o.leaf_per_lane ? 0 : 1;
   a.nl1 = g->nl1;
   a.n = (int32_t)g->n;
   a.nplans = nplans;
