@@ -435,15 +435,15 @@ def run_learned(args, workload):
         roots = ctx.roots(g, p)
         score = learn.page_scores(hg.rowptr, roots, torch.expm1(pred[:, 1].clamp_min(0)).cpu().numpy(),
                                   w["paged"]["page_bytes"] // 4, info["n_pages"])
-    kw = dict(timeout_ms=args.timeout_s * 1000, cold_cache=bool(w.get("paged")))
+    kw = dict(timeout_ms=args.timeout_s * 1000)
     res = {}
     for mode in ("plain", "learned"):
-        if mode == "learned" and w.get("paged"):
-            import numpy as np
-            g.set_resident_pages(np.argsort(-score)[:info["n_frames"]])
+        if w.get("paged"):
+            # plain: the first pages of the array (the reference's device
+            # partition); learned: the pages the model predicts hottest
+            pages = np.arange(info["n_frames"]) if mode == "plain" else np.argsort(-score)[:info["n_frames"]]
+            g.set_resident_pages(pages)
         extra = dict(root_order_ptr=order.data_ptr()) if mode == "learned" else {}
-        if mode == "learned" and w.get("paged"):
-            extra["cold_cache"] = False
         times, stats = [], None
         for k in range(args.warmup + args.steps):
             c, stt = ctx.match(g, [p], **kw, **extra)

@@ -405,38 +405,33 @@ class Context:
 
     @staticmethod
     def _opts(**kw) -> RunOpts:
+        """pm_run_opts from keyword arguments named after its fields (device
+        pointers as <field>_ptr); an unknown name is a TypeError."""
         o = RunOpts()
         lib().pm_run_opts_default(C.byref(o))
+        fields = {name for name, _ in RunOpts._fields_ if not name.endswith("_")}
         for k, v in kw.items():
+            name = k[:-4] if k.endswith("_ptr") else k
+            if name not in fields:
+                raise TypeError(f"unknown run option {k!r}")
             if k.endswith("_ptr"):
-                setattr(o, k[:-4], v or None)
+                setattr(o, name, v or None)
             else:
-                setattr(o, k, int(v))
+                setattr(o, name, int(v))
         return o
 
     def prepare(self, g: GraphPreprocessor, patterns: Sequence[PatternPreprocessor], **kw) -> "Query":
         """A prepared batched launch replayed from a CUDA graph (pm_query_*)."""
         return Query(self, g, patterns, self._opts(**kw))
 
-    def match(self, g: GraphPreprocessor, patterns: Sequence[PatternPreprocessor], *, truncate: int = 0,
-              warps_per_block: int = 0, blocks_per_sm: int = 0, chunk: int = 0, split_level1: int = 0,
-              shard_rank: int = 0, shard_count: int = 0, root_begin: int = -1, root_end: int = -1,
-              root_counts_ptr: int = 0, root_cost_ptr: int = 0, root_order_ptr: int = 0, root_reads_ptr: int = 0,
-              use_graph: bool = False, timeout_ms: int = 0, cold_cache: bool = False,
-              high_occupancy: int = 0):
-        """Runs all patterns in one launch; returns (counts list, stats dict)."""
-        o = RunOpts()
-        lib().pm_run_opts_default(C.byref(o))
-        o.truncate, o.warps_per_block, o.blocks_per_sm, o.chunk = truncate, warps_per_block, blocks_per_sm, chunk
-        o.split_level1, o.shard_rank, o.shard_count = split_level1, shard_rank, shard_count
-        o.root_begin, o.root_end, o.use_graph = root_begin, root_end, int(use_graph)
-        o.timeout_ms = timeout_ms
-        o.cold_cache = int(cold_cache)
-        o.high_occupancy = int(high_occupancy)
-        o.root_counts = root_counts_ptr or None
-        o.root_cost = root_cost_ptr or None
-        o.root_order = root_order_ptr or None
-        o.root_reads = root_reads_ptr or None
+    def match(self, g: GraphPreprocessor, patterns: Sequence[PatternPreprocessor], **kw):
+        """Runs all patterns in one launch; returns (counts list, stats dict).
+        Keyword arguments are pm_run_opts fields (truncate, warps_per_block,
+        chunk, split_level1, shard_rank/shard_count, root_begin/root_end,
+        timeout_ms, cold_cache, high_occupancy, leaf_per_lane, use_graph) and
+        device pointers root_counts_ptr, root_cost_ptr, root_order_ptr,
+        root_reads_ptr."""
+        o = self._opts(**kw)
         k = len(patterns)
         arr = (C.c_void_p * k)(*[p._h.value for p in patterns])
         counts = (C.c_uint64 * k)()
