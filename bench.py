@@ -352,7 +352,7 @@ def run_ours(args, workload):
             "data": "synthetic",
             "config": {"workload": workload, "graph": w["graph"], "labeled": w["labeled"],
                        "patterns": [p for p, _ in texts], "counts": counts_total,
-                       "kernel_variant": ["default", "regs64", "regs85"][args.high_occupancy] +
+                       "kernel_variant": ["default", "regs64", "regs85", "uncapped"][args.high_occupancy] +
                                          ("+leaf_per_lane" if args.leaf_per_lane else ""),
                        "root_limit": args.root_limit or None,
                        "roots": int(st["n_roots"]), "set_ops_per_step": set_ops // args.steps,
@@ -521,7 +521,7 @@ def main():
     ap.add_argument("--timeout-s", type=int, default=120, help="hard device-side limit per launch")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--high-occupancy", type=int, default=0,
-                    help="kernel variant: 0 no register cap, 1 capped at 64, 2 capped at 85")
+                    help="kernel variant: 0 default, 1 capped at 64 registers, 2 capped at 85, 3 uncapped")
     ap.add_argument("--leaf-per-lane", action="store_true",
                     help="last level one candidate per lane instead of work-balanced across the warp")
     ap.add_argument("--root-limit", type=int, default=0, help="profile this many roots only (from --root-begin)")

@@ -1733,17 +1733,23 @@ static pm_status setup_launch(pm_ctx* c, const pm_graph* g, const pm_plan* const
   // launch geometry: persistent, occupancy-limited
   L->threads = wpb * 32;
   L->smem = sizeof(WarpState) * wpb;
-  if (o.high_occupancy == 2) {
-    if (wpb > 8) return fail(PM_ERR_INVALID, "warps_per_block 16 is not available with high_occupancy");
-    L->kfn = L->labeled ? (L->paged ? match_kernel<true, true, 3> : match_kernel<true, false, 3>)
-                        : (L->paged ? match_kernel<false, true, 3> : match_kernel<false, false, 3>);
-  } else if (!o.high_occupancy) {
-    L->kfn = L->labeled ? (L->paged ? match_kernel<true, true, 1> : match_kernel<true, false, 1>)
-                        : (L->paged ? match_kernel<false, true, 1> : match_kernel<false, false, 1>);
-  } else {
-    if (wpb > 8) return fail(PM_ERR_INVALID, "warps_per_block 16 is not available with high_occupancy");
+  // kernel variant by register cap: 85 registers (three 256-thread blocks per
+  // SM) measures fastest on HBM graphs; paged graphs and 16-warp blocks use
+  // the uncapped variant unless one is asked for
+  int variant = o.high_occupancy;
+  if (variant == 0) variant = (!L->paged && wpb <= 8) ? 2 : 3;
+  if (variant < 0 || variant > 3) return fail(PM_ERR_INVALID, "high_occupancy must be 0..3");
+  if ((variant == 1 || variant == 2) && wpb > 8)
+    return fail(PM_ERR_INVALID, "warps_per_block 16 needs the uncapped kernel variant (high_occupancy 3)");
+  if (variant == 1) {
     L->kfn = L->labeled ? (L->paged ? match_kernel<true, true, 4> : match_kernel<true, false, 4>)
                         : (L->paged ? match_kernel<false, true, 4> : match_kernel<false, false, 4>);
+  } else if (variant == 2) {
+    L->kfn = L->labeled ? (L->paged ? match_kernel<true, true, 3> : match_kernel<true, false, 3>)
+                        : (L->paged ? match_kernel<false, true, 3> : match_kernel<false, false, 3>);
+  } else {
+    L->kfn = L->labeled ? (L->paged ? match_kernel<true, true, 1> : match_kernel<true, false, 1>)
+                        : (L->paged ? match_kernel<false, true, 1> : match_kernel<false, false, 1>);
   }
   int per_sm = 0;
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, L->kfn, L->threads, L->smem));

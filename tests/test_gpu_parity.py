@@ -146,7 +146,7 @@ def test_gpu_launch_shapes(ctx, wpb, chunk):
         text = PATTERNS[pname]
         want, st = oracle_count(hg, text, False)
         for split in (-1, 1, 8):
-            for high in ((False,) if wpb == 16 else (False, True)):
+            for high in ((0, 3) if wpb == 16 else (0, 1, 2, 3)):
                 got, gst = ctx.match(g, [pm.PatternPreprocessor(text=text, labeled=False)], warps_per_block=wpb,
                                      chunk=chunk, split_level1=split, high_occupancy=high)
                 assert got[0] == want, (pname, wpb, chunk, split, high)
