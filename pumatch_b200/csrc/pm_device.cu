@@ -190,7 +190,7 @@ __device__ __forceinline__ ListRef adj(const MatchArgs& a, WarpState& S, int v, 
   const int len = (int)(a.rowptr[v + 1] - b);
   w.reads++;
   if (!PAGED) return ListRef{a.colidx + b, len, -1};
-  if (a.host_sorted) return ListRef{a.host_sorted + b, len, -1};
+  if (a.host_sorted) return host_list_copy(a.host_sorted + b, len, gather);
   return paged_list(a.pg, b, len, gather, S.pins, w.pc);
 }
 
@@ -663,10 +663,21 @@ __device__ unsigned long long leaf_batch(const MatchArgs& a, const DPlan& P, War
               cgl = f >= a.pg.n_static;
               lpc.hits++;
             } else if (p0 == p1 && gr.y <= PM_LANE_MAX) {
-              // a short list on a missing page: this lane reads it from host
-              // memory (a warp keeps 32 such reads in flight) and asks for the page
+              // a short list on a missing page: this lane copies it from host
+              // memory into its own part of the gather space, 16 reads in
+              // flight per round trip, and asks for the page
               if (ld_vol(&a.pg.page_frame[p0]) == PAGE_ABSENT) request_page(a.pg, p0, lpc);
-              A = a.pg.host_colidx + s0;
+              const int32_t* src = a.pg.host_colidx + s0;
+              int32_t* stage = arena + a.slot_words + lane * PM_LANE_MAX;
+              for (int x = 0; x < gr.y; x += 16) {
+                int v[16];
+#pragma unroll
+                for (int q = 0; q < 16; q++) v[q] = (x + q < gr.y) ? src[x + q] : 0;
+#pragma unroll
+                for (int q = 0; q < 16; q++)
+                  if (x + q < gr.y) stage[x + q] = v[q];
+              }
+              A = stage;
               lpc.misses++;
               lpc.zc_bytes += 4ull * (unsigned long long)gr.y;
             } else {
@@ -1728,7 +1739,9 @@ static pm_status setup_launch(pm_ctx* c, const pm_graph* g, const pm_plan* const
     L->dp[i].nroots = e - b;
   }
   const int64_t slot_words = arena_words;
-  if (L->paged) arena_words += 2 * (int64_t)g->maxdeg + 64;  // gather space for multi-page lists
+  // gather space for multi-page lists (two operands), at least a short list
+  // per lane for the last level's copies of lists on missing pages
+  if (L->paged) arena_words += std::max<int64_t>(2 * (int64_t)g->maxdeg + 64, 32 * PM_LANE_MAX);
 
   // launch geometry: persistent, occupancy-limited
   L->threads = wpb * 32;

@@ -136,12 +136,34 @@ struct ListRef {
   bool cg;         // an evictable frame: read through L2 only (refilled during the launch)
 };
 
+// Copies a list out of mapped host memory into gather (whole warp), eight
+// reads in flight per lane (one round trip per 256 entries), so that the set
+// operation runs on device memory.
+__device__ __forceinline__ ListRef host_list_copy(const int32_t* src, int len, int32_t* gather) {
+  const int lane = threadIdx.x & 31;
+  for (int base = 0; base < len; base += 256) {
+    int v[8];
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+      const int i = base + q * 32 + lane;
+      v[q] = i < len ? src[i] : 0;
+    }
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+      const int i = base + q * 32 + lane;
+      if (i < len) gather[i] = v[q];
+    }
+  }
+  __syncwarp();
+  return ListRef{gather, len, -1};
+}
+
 // Most pages one list may span and still be gathered from frames; longer
 // lists are read from host memory.
 #define PM_MAX_LIST_PAGES 64
 
 // Resolves the adjacency list [b, b+len) of colidx for the whole warp.
-// gather: arena space for a multi-page list (>= len words); pins: per-warp
+// gather: arena space for a copied list (>= len words); pins: per-warp
 // shared scratch of PM_MAX_LIST_PAGES frame indices.  Frames are remembered
 // from the pin, never re-read from the table (an evictor can hold an entry at
 // PAGE_EVICTING for a moment even while the frame is pinned).
@@ -185,7 +207,7 @@ static __device__ ListRef paged_list(const DPaging& pg, uint64_t b, int len, int
     const uint64_t off = b & ((1ull << sh) - 1);
     return ListRef{pg.frames + ((uint64_t)f0 << sh) + off, len, f0, f0 >= pg.n_static};
   }
-  if (mode == 1) return ListRef{pg.host_colidx + b, len, -1};
+  if (mode == 1) return host_list_copy(pg.host_colidx + b, len, gather);
   // gather the pinned pages into the arena, then unpin them
   __syncwarp();
   const uint64_t e = b + (uint64_t)len;
