@@ -232,7 +232,11 @@ typedef struct {
                                lane (long lists go to the warp); 0 (default):
                                work-balanced across the warp when the common
                                operand fits in shared memory                 */
-  int32_t reserved_;
+  int32_t lane_subtree_max; /* unlabeled plans ending in a chain of
+                               intersections (cliques): the last two levels
+                               run one candidate per lane when the parent set
+                               is at most this long; 0 = default (64), -1 =
+                               never                                          */
   uint64_t* root_counts;    /* optional device ptr: per-root counts (plan 0) */
   float* root_cost;         /* optional device ptr: per-root set-op bytes    */
   const int32_t* root_order;/* optional device ptr: process roots in this

@@ -63,7 +63,7 @@ class RunOpts(C.Structure):
                 ("chunk", C.c_int32), ("split_level1", C.c_int32), ("shard_rank", C.c_int32),
                 ("shard_count", C.c_int32), ("use_graph", C.c_int32), ("timeout_ms", C.c_int32),
                 ("root_begin", C.c_int64), ("root_end", C.c_int64), ("cold_cache", C.c_int32),
-                ("high_occupancy", C.c_int32), ("leaf_per_lane", C.c_int32), ("reserved_", C.c_int32),
+                ("high_occupancy", C.c_int32), ("leaf_per_lane", C.c_int32), ("lane_subtree_max", C.c_int32),
                 ("root_counts", C.c_void_p), ("root_cost", C.c_void_p), ("root_order", C.c_void_p),
                 ("root_reads", C.c_void_p)]
 
@@ -428,7 +428,7 @@ class Context:
         """Runs all patterns in one launch; returns (counts list, stats dict).
         Keyword arguments are pm_run_opts fields (truncate, warps_per_block,
         chunk, split_level1, shard_rank/shard_count, root_begin/root_end,
-        timeout_ms, cold_cache, high_occupancy, leaf_per_lane, use_graph) and
+        timeout_ms, cold_cache, high_occupancy, leaf_per_lane, lane_subtree_max, use_graph) and
         device pointers root_counts_ptr, root_cost_ptr, root_order_ptr,
         root_reads_ptr."""
         o = self._opts(**kw)

@@ -77,7 +77,7 @@ struct MatchArgs {
   const int32_t* lab_off;       // label group offsets (labeled, HBM or paged) or null
   const int32_t* host_sorted;   // labeled paged: the id-sorted lists in mapped host memory
   int32_t leaf_flat;            // last-level intersections work-balanced across the warp (leaf_flat)
-  int32_t pad2;
+  int32_t lane_subtree_max;     // lane_subtree when the parent set is at most this long; 0 = never
   int32_t nl1;
   int32_t pad1;
   int32_t n;
@@ -438,14 +438,15 @@ __device__ __forceinline__ int lane_lower_bound(const int32_t* A, int len, int x
 // (usually in shared memory), galloping through B; four loads of A in
 // flight.  Sets *lenA to the number of elements of A below ub (the
 // reference's scan length) and returns the count of members (label-checked
-// when LABELED), or -1 when more than PM_LANE_MAX elements would be scanned
-// (the caller hands the candidate to the whole warp).
+// when LABELED), or -1 when more than `cap` elements would be scanned (the
+// caller hands the candidate to the whole warp).
 template <bool LABELED, bool CG>
 __device__ __forceinline__ int lane_intersect(const int32_t* A, int deg, int ub, const int32_t* B, int lenB,
-                                              const uint8_t* labels, uint32_t mask, int* lenA, bool cg) {
+                                              const uint8_t* labels, uint32_t mask, int* lenA, bool cg,
+                                              int cap = PM_LANE_MAX) {
   int k = 0, p = 0, x = 0;
   while (true) {
-    if (x >= PM_LANE_MAX) return -1;
+    if (x >= cap) return -1;
     int v[4];
 #pragma unroll
     for (int q = 0; q < 4; q++) v[q] = (x + q < deg) ? ld<CG>(A + x + q, cg) : INT_MAX;
@@ -809,6 +810,105 @@ __device__ unsigned long long leaf_batch(const MatchArgs& a, const DPlan& P, War
   return cnt + cnt_warp;
 }
 
+// The last two levels below candidates [b, e) of level L = nnodes-4, one
+// lane per candidate v: the lane computes level L+1's intersection X (and
+// its alias Y) for path[L+1] = v into its own part of the free arena, then
+// counts the last level over X/Y's candidates -- the small sets of light
+// subtrees, where warp-wide set operations leave most lanes idle.  Same set
+// operations, counts and accounting as run_level + leaf_batch; unlabeled
+// plans of the shape DPlan.l2_x describes, no truncation, X's parent at most
+// lane_subtree_max long (it is staged in shared memory).
+__device__ unsigned long long lane_subtree(const MatchArgs& a, const DPlan& P, WarpState& S, int32_t* arena,
+                                           int L, int b, int e, Work& w) {
+  const int lane = lane_id();
+  const int Lq = L + 1;
+  const int X = P.l2_x, Y = P.l2_y, M = P.level_begin[Lq], last = P.last_slot;
+  const int p1 = P.parent[X];
+  const int lenB1 = S.size[p1];
+  const int32_t* B1 = arena + S.off[p1];
+  for (int i = lane; i < lenB1; i += 32) S.sb[i] = B1[i];
+  __syncwarp();
+  const int32_t* Bs = S.sb;
+  const int32_t* cand = arena + S.off[P.level_begin[L]];
+  unsigned long long cnt = 0, bytes = 0, ops = 0;
+  const int i = b + lane;
+  if (i < e) {
+    const int v = cand[i];
+    // slot bounds with path[Lq] = v: main slots take the smallest constrained
+    // path vertex, helpers the largest (slot_bound)
+    auto bound = [&](int s) -> int {
+      const bool is_main = (s == M);
+      long long ub = is_main ? INT_MAX : -1;
+      for (int j = 0; j <= Lq; j++) {
+        if (!((P.partial[s] >> j) & 1u)) continue;
+        const long long pv = (j == Lq) ? v : S.path[j];
+        if (is_main) { if (pv <= ub) ub = pv; }
+        else if (ub < pv) ub = pv;
+      }
+      return ub == -1 ? INT_MAX : (int)ub;
+    };
+    const uint64_t rb = a.rowptr[v];
+    const int deg = (int)(a.rowptr[v + 1] - rb);
+    const int32_t* A = a.colidx + rb;
+    // X = N(v) below its bound, intersected with its parent
+    const int ubX = bound(X);
+    const int lenAX = (ubX == INT_MAX) ? deg : lane_lower_bound(A, deg, ubX);
+    int32_t* buf = arena + S.top[Lq] + lane * lenB1;
+    int sizeX = 0, p = 0;
+    for (int x = 0; x < lenAX && p < lenB1; x++) {
+      const int val = A[x];
+      int lo = p, step = 1;
+      while (lo + step < lenB1 && Bs[lo + step] < val) { lo += step; step <<= 1; }
+      int hi = min(lo + step + 1, lenB1);
+      while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (Bs[mid] < val) lo = mid + 1; else hi = mid;
+      }
+      p = lo;
+      if (p < lenB1 && Bs[p] == val) buf[sizeX++] = val;
+    }
+    bytes += 4ull * (unsigned long long)(lenAX + lenB1 + sizeX);
+    ops++;
+    w.reads++;
+    // Y: X itself or its prefix below Y's bound, charged as its own operation
+    int sizeY = sizeX;
+    if (Y >= 0) {
+      const int ubY = bound(Y);
+      if (P.alias_prefix[Y] && ubY != INT_MAX) sizeY = lane_lower_bound(buf, sizeX, ubY);
+      const int lenAY = (ubY == INT_MAX) ? deg : lane_lower_bound(A, deg, ubY);
+      bytes += 4ull * (unsigned long long)(lenAY + lenB1 + sizeY);
+      ops++;
+    }
+    const int sizeM = (M == X) ? sizeX : sizeY;
+    const int sizeB = (P.parent[last] == X) ? sizeX : sizeY;
+    // the last level over the main slot's candidates c
+    int common = INT_MAX;
+    for (int j = 0; j <= Lq; j++)
+      if ((P.partial[last] >> j) & 1u) common = min(common, (j == Lq) ? v : S.path[j]);
+    const bool self_ub = (P.partial[last] >> (Lq + 1)) & 1u;
+    for (int k = 0; k < sizeM; k++) {
+      const int c = buf[k];
+      const int ub = self_ub ? min(common, c) : common;
+      const uint64_t rc = a.rowptr[c];
+      const int dc = (int)(a.rowptr[c + 1] - rc);
+      int lenA = 0;
+      const int kk = lane_intersect<false, false>(a.colidx + rc, dc, ub, buf, sizeB, a.labels, 0u, &lenA, false,
+                                                  INT_MAX);
+      cnt += (unsigned long long)kk;
+      bytes += 4ull * (unsigned long long)(lenA + sizeB + kk);
+      ops++;
+    }
+  }
+  for (int o = 16; o; o >>= 1) {
+    cnt += __shfl_xor_sync(FULL, cnt, o);
+    bytes += __shfl_xor_sync(FULL, bytes, o);
+    ops += __shfl_xor_sync(FULL, ops, o);
+  }
+  w.setops += ops;
+  w.bytes += bytes;
+  return cnt;
+}
+
 // A donated piece of a DFS: candidates [begin, end) of level `level`'s main
 // slot under the path root(v0, v1), path[2..level].
 struct Donation {
@@ -900,7 +1000,17 @@ __device__ unsigned long long dfs_from(const MatchArgs& a, const DPlan& P, WarpS
     const int m = P.level_begin[L];
     const int it = S.iter[L];
     const int iend = S.iend[L];
-    if (it < iend && L + 1 == n - 2) {
+    bool subtree = false;
+    if constexpr (!LABELED && !PAGED)
+      subtree = P.l2_x >= 0 && L + 4 == n && it < iend && a.lane_subtree_max > 0 &&
+                S.size[P.parent[P.l2_x]] <= a.lane_subtree_max &&
+                S.top[L + 1] + 32ll * S.size[P.parent[P.l2_x]] <= a.slot_words;
+    if (subtree) {
+      const int e2 = min(iend, it + 32);
+      cnt += lane_subtree(a, P, S, arena, L, it, e2, w);
+      if (lane == 0) S.iter[L] = e2;
+      __syncwarp();
+    } else if (it < iend && L + 1 == n - 2) {
       const int e2 = min(iend, it + PM_LEAF_BATCH);
       cnt += leaf_batch<LABELED, PAGED>(a, P, S, arena, L, it, e2, w);
       if (lane == 0) S.iter[L] = e2;
@@ -1287,6 +1397,26 @@ DPlan to_dplan(const Plan& p) {
         d.alias_prefix[s] = (s == b) ? 1 : 0;
         break;
       }
+    }
+  }
+  // Shape for lane_subtree (unlabeled): level n-3 is one intersection X with
+  // a parent at an earlier level, plus at most one alias Y of it; the last
+  // slot intersects with X or Y.
+  d.l2_x = d.l2_y = -1;
+  const int n = p.nnodes;
+  if (!p.labeled && n >= 5) {
+    const int b = p.level_begin[n - 3], e = p.level_begin[n - 2];
+    int x = -1, y = -1, others = 0;
+    for (int s = b; s < e; s++) {
+      if (d.alias[s] < 0) { if (x < 0) x = s; else others++; }
+      else if (y < 0) y = s;
+      else others++;
+    }
+    const int last = d.last_slot;
+    if (x >= 0 && !others && (y < 0 || d.alias[y] == x) && d.kind[x] == SLOT_INTERSECT && d.parent[x] < b &&
+        d.kind[last] == SLOT_INTERSECT && (d.parent[last] == x || (y >= 0 && d.parent[last] == y))) {
+      d.l2_x = (int8_t)x;
+      d.l2_y = (int8_t)y;
     }
   }
   return d;
@@ -1795,6 +1925,7 @@ static pm_status setup_launch(pm_ctx* c, const pm_graph* g, const pm_plan* const
   a.lab_off = g->d_lab_off;
   a.host_sorted = (g->residency == PM_RESIDENT_PAGED && g->d_lab_off) ? g->h_colidx_dev : nullptr;
   a.leaf_flat = o.leaf_per_lane ? 0 : 1;
+  a.lane_subtree_max = o.lane_subtree_max < 0 ? 0 : (o.lane_subtree_max == 0 ? 64 : std::min(o.lane_subtree_max, PM_SB_MAX));
   a.nl1 = g->nl1;
   a.n = (int32_t)g->n;
   a.nplans = nplans;

@@ -34,6 +34,11 @@ struct DPlan {
                                   // same operation whose result contains this one
   uint8_t alias_prefix[16];       // 1: this slot is the alias's prefix below
                                   // this slot's own bound; 0: equal sets
+  // last two levels one lane per candidate (lane_subtree): the computed
+  // intersection of level nnodes-3, its alias (or -1); l2_x = -1 when the
+  // plan does not have that shape
+  int8_t l2_x, l2_y;
+  int8_t pad_[6];
   const int2* roots;              // (v0, v1) root edges, reference order
   int64_t nroots;
 };

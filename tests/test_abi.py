@@ -114,11 +114,12 @@ def test_run_option_keywords():
     silently ignored attribute."""
     o = pm.Context._opts(truncate=4, warps_per_block=8, blocks_per_sm=2, chunk=7, split_level1=16, shard_rank=1,
                          shard_count=2, root_begin=3, root_end=9, timeout_ms=1000, cold_cache=True,
-                         high_occupancy=2, leaf_per_lane=1, use_graph=True, root_counts_ptr=0,
+                         high_occupancy=2, leaf_per_lane=1, lane_subtree_max=-1, use_graph=True, root_counts_ptr=0,
                          root_cost_ptr=0, root_order_ptr=0, root_reads_ptr=0)
     assert (o.truncate, o.chunk, o.root_begin, o.root_end, o.leaf_per_lane, o.high_occupancy) == (4, 7, 3, 9, 1, 2)
     assert o.cold_cache == 1 and o.use_graph == 1 and o.root_order is None
     d = pm.Context._opts()
-    assert d.root_begin == -1 and d.root_end == -1 and d.leaf_per_lane == 0
+    assert d.root_begin == -1 and d.root_end == -1 and d.leaf_per_lane == 0 and d.lane_subtree_max == 0
+    assert o.lane_subtree_max == -1
     with pytest.raises(TypeError):
         pm.Context._opts(leaf_mode=1)

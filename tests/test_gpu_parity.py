@@ -75,20 +75,29 @@ COUNT_PATTERNS = ["cycle4", "cycle5", "clique4", "clique5", "path4", "path5", "s
                   "path5_lab", "house_lab", "cycle5_tail2_lab", "clique4_lab", "star5_lab"]
 
 
+MODES = {"default": {}, "perlane": {"leaf_per_lane": 1}, "nosubtree": {"lane_subtree_max": -1},
+         "subtree512": {"lane_subtree_max": 512}}
+
+
 @pytest.mark.parametrize("gname", GRAPHS)
 @pytest.mark.parametrize("labeled", [True, False], ids=["lab", "unl"])
-@pytest.mark.parametrize("per_lane", [0, 1], ids=["balanced", "perlane"])
-def test_gpu_counts_match_oracle(ctx, gname, labeled, per_lane):
-    """Both last-level schemes (work-balanced across the warp, one candidate
-    per lane) give the oracle's counts, set operations and bytes."""
+@pytest.mark.parametrize("mode", sorted(MODES))
+def test_gpu_counts_match_oracle(ctx, gname, labeled, mode):
+    """Every last-level scheme (work-balanced across the warp, one candidate
+    per lane, the last two levels one candidate per lane for clique-like
+    plans at any parent size or never) gives the oracle's counts, set
+    operations and bytes."""
+    if labeled and mode in ("nosubtree", "subtree512"):
+        pytest.skip("the two-level lane scheme is for unlabeled plans only")
     hg = host_graph(gname, labeled)
     g = dev_graph(gname, labeled)
-    for pname in COUNT_PATTERNS:
+    names = COUNT_PATTERNS + ([] if labeled else ["clique6", "clique7"])
+    for pname in names:
         if not labeled and pname.startswith("cycle5_tail2"):
             continue  # minutes of oracle time unlabeled; covered labeled and on the small graphs
         text = PATTERNS[pname]
         want, st = oracle_count(hg, text, labeled)
-        got, gst = ctx.match(g, [pm.PatternPreprocessor(text=text, labeled=labeled)], leaf_per_lane=per_lane)
+        got, gst = ctx.match(g, [pm.PatternPreprocessor(text=text, labeled=labeled)], **MODES[mode])
         assert got[0] == want, (gname, pname)
         assert gst["set_ops"] == st["set_ops"], (gname, pname)
         assert gst["alg_bytes"] == st["alg_bytes"], (gname, pname)
