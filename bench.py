@@ -265,7 +265,7 @@ def run_ours(args, workload):
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")  # > 126 MB L2
     shard = dict(shard_rank=rank, shard_count=world) if world > 1 else {}
     run_kw = dict(timeout_ms=args.timeout_s * 1000, high_occupancy=args.high_occupancy,
-                  leaf_per_lane=int(args.leaf_per_lane), **shard)
+                  leaf_per_lane=int(args.leaf_per_lane), lane_subtree_max=args.lane_subtree_max, **shard)
     if args.root_limit > 0:
         run_kw.update(root_begin=args.root_begin, root_end=args.root_begin + args.root_limit)
 
@@ -353,7 +353,9 @@ def run_ours(args, workload):
             "config": {"workload": workload, "graph": w["graph"], "labeled": w["labeled"],
                        "patterns": [p for p, _ in texts], "counts": counts_total,
                        "kernel_variant": ["default", "regs64", "regs85", "uncapped"][args.high_occupancy] +
-                                         ("+leaf_per_lane" if args.leaf_per_lane else ""),
+                                         ("+leaf_per_lane" if args.leaf_per_lane else "") +
+                                         (f"+lane_subtree_max={args.lane_subtree_max}"
+                                          if args.lane_subtree_max else ""),
                        "root_limit": args.root_limit or None,
                        "roots": int(st["n_roots"]), "set_ops_per_step": set_ops // args.steps,
                        "donated_ranges_last_step": int(st["splits"]),
@@ -524,6 +526,9 @@ def main():
                     help="kernel variant: 0 default, 1 capped at 64 registers, 2 capped at 85, 3 uncapped")
     ap.add_argument("--leaf-per-lane", action="store_true",
                     help="last level one candidate per lane instead of work-balanced across the warp")
+    ap.add_argument("--lane-subtree-max", type=int, default=0,
+                    help="clique-like plans: last two levels one candidate per lane up to this parent size "
+                         "(0 default, -1 never)")
     ap.add_argument("--root-limit", type=int, default=0, help="profile this many roots only (from --root-begin)")
     ap.add_argument("--root-begin", type=int, default=0)
     ap.add_argument("--learned", action="store_true", help="plain vs learned scheduling on the workload")
