@@ -1877,10 +1877,9 @@ static pm_status setup_launch(pm_ctx* c, const pm_graph* g, const pm_plan* const
   L->threads = wpb * 32;
   L->smem = sizeof(WarpState) * wpb;
   // kernel variant by register cap: 85 registers (three 256-thread blocks per
-  // SM) measures fastest on HBM graphs; paged graphs and 16-warp blocks use
-  // the uncapped variant unless one is asked for
+  // SM) measures fastest; 16-warp blocks need the uncapped variant
   int variant = o.high_occupancy;
-  if (variant == 0) variant = (!L->paged && wpb <= 8) ? 2 : 3;
+  if (variant == 0) variant = (wpb <= 8) ? 2 : 3;
   if (variant < 0 || variant > 3) return fail(PM_ERR_INVALID, "high_occupancy must be 0..3");
   if ((variant == 1 || variant == 2) && wpb > 8)
     return fail(PM_ERR_INVALID, "warps_per_block 16 needs the uncapped kernel variant (high_occupancy 3)");
