@@ -223,11 +223,10 @@ typedef struct {
   int64_t root_end;
   int32_t cold_cache;       /* paged mode: empty the frame pool before the run */
   int32_t high_occupancy;   /* kernel variant by register cap: 0 default (85
-                               on graphs in HBM with <= 8 warps per block,
-                               else uncapped); 1 capped at 64 registers (four
-                               256-thread blocks per SM); 2 capped at 85
-                               (three blocks per SM); 3 uncapped (up to 128,
-                               no spills)                                    */
+                               with <= 8 warps per block, else uncapped); 1
+                               capped at 64 registers (four 256-thread
+                               blocks per SM); 2 capped at 85 (three blocks
+                               per SM); 3 uncapped (up to 128, no spills)    */
   int32_t leaf_per_lane;    /* 1: last-level intersections one candidate per
                                lane (long lists go to the warp); 0 (default):
                                work-balanced across the warp when the common
