@@ -1,6 +1,6 @@
 """Autotuner for the batched persistent launch.
 
-Sweeps warps per block, root chunk size, level-1 split threshold and -- for
+Sweeps warps per block, root chunk size, donation threshold and -- for
 paged graphs -- page size, timing each configuration with the device time the
 library reports, and keeps the fastest per (graph, pattern set).  Every
 configuration must return the same counts; a mismatch is an error, never a

@@ -7,17 +7,21 @@
 //   * work = root edges (v0, v1) of one or more plans, handed out in chunks
 //     by 64-bit atomic cursors (one per plan, warps start on different plans
 //     so a batch of patterns interleaves);
-//   * a warp that still has a large level-1 candidate range when the queue
-//     has run dry donates the upper half of that range to a global donation
-//     ring that idle warps drain (replaces the reference's disabled
-//     stealing, src/gpu_match.cu:21-148, 818-853);
+//   * a warp that still holds a candidate range (at any DFS level) when the
+//     queue has run dry donates the upper half of its shallowest splittable
+//     range, with the path prefix, to a global donation ring that idle warps
+//     drain (replaces the reference's disabled stealing,
+//     src/gpu_match.cu:21-148, 818-853);
 //   * each level's candidate sets ("slots") are computed by a warp-cooperative
 //     sorted-set operation -- 32 candidates per step, per-lane membership
 //     search, __ballot_sync/__popc compaction -- and stored in a per-warp
 //     arena in HBM sized to the plan's worst case, so nothing is truncated
 //     (the reference caps every set at GRAPH_DEGREE=4096; that cap is kept
 //     only as an explicit emulation switch);
-//   * the last level is counted, never materialised.
+//   * the last level is counted, never materialised: work-balanced across
+//     the warp (leaf_flat), one candidate per lane (leaf_batch), or, for
+//     clique-like plans, the last two levels one candidate per lane
+//     (lane_subtree).
 #include <cub/cub.cuh>
 #include <cuda_runtime.h>
 
@@ -1141,7 +1145,7 @@ __global__ void __launch_bounds__(MINB == 1 ? 512 : 256, MINB) match_kernel(Matc
     if (lane == 0 && local) atomicAdd(&a.counts[p], local);
     p = (p + 1 == np) ? 0 : p + 1;  // interleave plans chunk by chunk
   }
-  // phase 2: drain donated level-1 ranges until no warp holds work
+  // phase 2: drain donated ranges until no warp holds work
   __threadfence();
   if (lane == 0) atomicSub(a.active, 1u);
   __syncwarp();
