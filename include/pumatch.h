@@ -129,6 +129,26 @@ void pm_host_free(void* p);
 pm_status pm_convert_snap(const char* snap_path, const char* out_prefix, int n_labels,
                           int keep_self_loops, int64_t* n_vertices, int64_t* n_adj);
 
+/* Degree order (graph_converter/relabel.cpp:26-63): vertices sorted by
+ * (degree, id), highest first, take new ids 0..n-1; lists are rewritten and
+ * sorted.  Counts of every pattern are unchanged (the graph is relabelled,
+ * not changed); clique searches, whose candidates lie below earlier path
+ * vertices, then scan the short lists of heavy vertices' lighter
+ * neighbours.  Outputs are caller-allocated: rowptr_out[n+1],
+ * colidx_out[n_adj], labels_out[n] (when labels), new_id_out[n] (optional:
+ * the new id of each old vertex).  Unlike relabel.cpp, labels move with
+ * their vertices. */
+pm_status pm_reorder_by_degree(int64_t n, int64_t n_adj, const uint64_t* rowptr, const int32_t* colidx,
+                               const uint32_t* labels, uint64_t* rowptr_out, int32_t* colidx_out,
+                               uint32_t* labels_out, int32_t* new_id_out);
+
+/* Half graph (graph_converter/halve.cpp:19-30): each undirected edge once,
+ * from the endpoint of lower degree to the higher (ties: to the higher id).
+ * colidx_out must hold n_adj entries; *n_adj_out receives the number used
+ * and *max_degree_out the longest half list. */
+pm_status pm_halve(int64_t n, int64_t n_adj, const uint64_t* rowptr, const int32_t* colidx,
+                   uint64_t* rowptr_out, int32_t* colidx_out, int64_t* n_adj_out, int32_t* max_degree_out);
+
 /* ------------------------------------------------------------------ */
 /* Synthetic inputs (stand-ins for the reference's converted datasets)  */
 /* ------------------------------------------------------------------ */

@@ -100,6 +100,8 @@ SIGNATURES = {
     "pm_host_free": (None, [_P]),
     "pm_convert_snap": (C.c_int, [C.c_char_p, C.c_char_p, C.c_int, C.c_int, C.POINTER(C.c_int64),
                                   C.POINTER(C.c_int64)]),
+    "pm_reorder_by_degree": (C.c_int, [C.c_int64, C.c_int64, _P, _P, _P, _P, _P, _P, _P]),
+    "pm_halve": (C.c_int, [C.c_int64, C.c_int64, _P, _P, _P, _P, C.POINTER(C.c_int64), C.POINTER(C.c_int32)]),
     "pm_gen_chung_lu": (C.c_int, [C.c_int64, C.c_int64, C.c_double, C.c_double, C.c_double, C.c_uint64,
                                   _PP, _PP, C.POINTER(C.c_int64), C.POINTER(C.c_int32)]),
     "pm_gen_rmat": (C.c_int, [C.c_int64, C.c_int64, C.c_double, C.c_double, C.c_double, C.c_uint64,
@@ -221,6 +223,31 @@ def convert_snap(snap_path: str, out_prefix: Optional[str] = None, n_labels: int
     _check(lib().pm_convert_snap(snap_path.encode(), (out_prefix or snap_path).encode(), n_labels,
                                  int(keep_self_loops), C.byref(n), C.byref(nadj)))
     return n.value, nadj.value
+
+
+def reorder_by_degree(hg: HostGraph):
+    """The same graph with vertices renumbered by (degree, id), highest first
+    (graph_converter/relabel.cpp); labels move with their vertices.  Returns
+    (HostGraph, new_id) where new_id[old] is the vertex's new id."""
+    rp = np.zeros(hg.n + 1, dtype=np.uint64)
+    ci = np.zeros(max(hg.n_adj, 1), dtype=np.int32)
+    lb = np.zeros(max(hg.n, 1), dtype=np.uint32) if hg.labels is not None else None
+    nid = np.zeros(max(hg.n, 1), dtype=np.int32)
+    _check(lib().pm_reorder_by_degree(hg.n, hg.n_adj, _ptr(hg.rowptr), _ptr(hg.colidx),
+                                      _ptr(hg.labels) if hg.labels is not None else None, _ptr(rp), _ptr(ci),
+                                      _ptr(lb) if lb is not None else None, _ptr(nid)))
+    return HostGraph(rp, ci[:hg.n_adj], None if lb is None else lb[:hg.n]), nid[:hg.n]
+
+
+def halve(hg: HostGraph):
+    """Each undirected edge once, towards its heavier end
+    (graph_converter/halve.cpp).  Returns (rowptr, colidx, max_degree)."""
+    rp = np.zeros(hg.n + 1, dtype=np.uint64)
+    ci = np.zeros(max(hg.n_adj, 1), dtype=np.int32)
+    nadj, md = C.c_int64(), C.c_int32()
+    _check(lib().pm_halve(hg.n, hg.n_adj, _ptr(hg.rowptr), _ptr(hg.colidx), _ptr(rp), _ptr(ci), C.byref(nadj),
+                          C.byref(md)))
+    return rp, ci[:nadj.value].copy(), md.value
 
 
 def gen_chung_lu(n: int, n_edges: int, gamma: float = 2.1, i0: float = 10.0, max_w: float = 5000.0,

@@ -500,6 +500,85 @@ extern "C" pm_status pm_graph_write(const char* prefix, int64_t n, int64_t nadj,
   return PM_OK;
 }
 
+// ------------------------------------------------- degree order and halving
+
+// Checks a CSR's shape: monotone offsets ending at n_adj, ids in range.
+static pm_status check_csr(const char* who, int64_t n, int64_t nadj, const uint64_t* rowptr,
+                           const int32_t* colidx) {
+  if (n < 0 || n > INT32_MAX || nadj < 0 || !rowptr || (nadj > 0 && !colidx))
+    return fail(PM_ERR_INVALID, "%s: bad arguments", who);
+  if (rowptr[0] != 0 || rowptr[n] != (uint64_t)nadj) return fail(PM_ERR_FORMAT, "%s: offsets do not span the lists", who);
+  for (int64_t v = 0; v < n; v++)
+    if (rowptr[v + 1] < rowptr[v]) return fail(PM_ERR_FORMAT, "%s: offsets of vertex %lld decrease", who, (long long)v);
+  for (int64_t i = 0; i < nadj; i++)
+    if (colidx[i] < 0 || colidx[i] >= n) return fail(PM_ERR_FORMAT, "%s: vertex id %d out of range", who, colidx[i]);
+  return PM_OK;
+}
+
+// Restates graph_converter/relabel.cpp:26-63: vertices sorted by (degree,
+// id) descending take the new ids 0, 1, ...; every list is rewritten in new
+// ids and sorted.  relabel.cpp copies no label file; here the labels move
+// with their vertices, so a labeled graph stays the same graph.
+extern "C" pm_status pm_reorder_by_degree(int64_t n, int64_t nadj, const uint64_t* rowptr, const int32_t* colidx,
+                                          const uint32_t* labels, uint64_t* rowptr_out, int32_t* colidx_out,
+                                          uint32_t* labels_out, int32_t* new_id_out) {
+  pm_status st = check_csr("pm_reorder_by_degree", n, nadj, rowptr, colidx);
+  if (st != PM_OK) return st;
+  if (!rowptr_out || (nadj > 0 && !colidx_out) || (labels && !labels_out))
+    return fail(PM_ERR_INVALID, "pm_reorder_by_degree: missing output");
+  std::vector<int32_t> order((size_t)n), nid((size_t)n);
+  for (int64_t v = 0; v < n; v++) order[v] = (int32_t)v;
+  auto deg = [&](int32_t v) { return rowptr[v + 1] - rowptr[v]; };
+  std::sort(order.begin(), order.end(), [&](int32_t x, int32_t y) {
+    const uint64_t dx = deg(x), dy = deg(y);
+    return dx != dy ? dx > dy : x > y;
+  });
+  for (int64_t i = 0; i < n; i++) nid[order[i]] = (int32_t)i;
+  rowptr_out[0] = 0;
+  for (int64_t i = 0; i < n; i++) rowptr_out[i + 1] = rowptr_out[i] + deg(order[i]);
+#pragma omp parallel for schedule(dynamic, 1024)
+  for (int64_t i = 0; i < n; i++) {
+    const int32_t old = order[i];
+    int32_t* out = colidx_out + rowptr_out[i];
+    const uint64_t b = rowptr[old], d = deg(old);
+    for (uint64_t k = 0; k < d; k++) out[k] = nid[colidx[b + k]];
+    std::sort(out, out + d);
+  }
+  if (labels)
+    for (int64_t i = 0; i < n; i++) labels_out[i] = labels[order[i]];
+  if (new_id_out) std::copy(nid.begin(), nid.end(), new_id_out);
+  return PM_OK;
+}
+
+// Restates graph_converter/halve.cpp:19-30: vertex u keeps neighbour w when
+// w has the higher degree, or the same degree and the higher id -- each
+// undirected edge once, towards its heavier end.  colidx_out must hold nadj
+// entries (exactly nadj/2 are used for a symmetric graph without loops).
+extern "C" pm_status pm_halve(int64_t n, int64_t nadj, const uint64_t* rowptr, const int32_t* colidx,
+                              uint64_t* rowptr_out, int32_t* colidx_out, int64_t* nadj_out,
+                              int32_t* max_degree_out) {
+  pm_status st = check_csr("pm_halve", n, nadj, rowptr, colidx);
+  if (st != PM_OK) return st;
+  if (!rowptr_out || (nadj > 0 && !colidx_out) || !nadj_out || !max_degree_out)
+    return fail(PM_ERR_INVALID, "pm_halve: missing output");
+  rowptr_out[0] = 0;
+  int64_t maxd = 0;
+  for (int64_t u = 0; u < n; u++) {
+    const uint64_t b = rowptr[u], e = rowptr[u + 1], du = e - b;
+    uint64_t o = rowptr_out[u];
+    for (uint64_t i = b; i < e; i++) {
+      const int32_t w = colidx[i];
+      const uint64_t dw = rowptr[w + 1] - rowptr[w];
+      if (dw > du || (dw == du && w > u)) colidx_out[o++] = w;
+    }
+    rowptr_out[u + 1] = o;
+    maxd = std::max<int64_t>(maxd, (int64_t)(o - rowptr_out[u]));
+  }
+  *nadj_out = (int64_t)rowptr_out[n];
+  *max_degree_out = (int32_t)maxd;
+  return PM_OK;
+}
+
 // ---------------------------------------------------------------- generators
 
 extern "C" pm_status pm_gen_chung_lu(int64_t n, int64_t m, double gamma, double i0, double max_w,
