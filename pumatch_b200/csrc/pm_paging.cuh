@@ -52,7 +52,8 @@ __device__ __forceinline__ void ring_post(const DPaging& pg, unsigned long long 
   *(volatile unsigned long long*)&pg.ring_seq[slot & pg.ring_mask] = slot + 1;
 }
 
-// Lane 0 only.  Starts loading page p if it is absent: reserve a ring slot,
+// One thread (lane 0 of a warp, or a lane for its own list).  Starts
+// loading page p if it is absent: reserve a ring slot,
 // claim the page, find a frame (never-used frames first, then a bounded
 // CLOCK sweep), post the request.  Never waits for the host.
 static __device__ void request_page(const DPaging& pg, int32_t p, PageCounters& pc) {
