@@ -298,3 +298,28 @@ def test_gpu_prepared_query_replays(ctx):
     p = pm.PatternPreprocessor(text=PATTERNS["cycle5"], labeled=False)
     q = ctx.prepare(gu, [p], warps_per_block=16, chunk=3)
     assert q.run()[0] == ctx.match(gu, [p])[0]
+
+
+def test_gpu_degree_order_keeps_counts(ctx):
+    """Renumbering by degree (the reference's relabel step) changes the
+    search, not the answer: every count is the same on the GPU and equals
+    the oracle's on the original graph."""
+    from pumatch_b200 import patterns as P
+    cases = {("cl3000", False): [PATTERNS["clique5"], PATTERNS["clique6"], PATTERNS["house"], PATTERNS["cycle5"]],
+             ("rmat512", True): [P.to_g(*P.house(), [0, 1, 0, 1, 0]), P.to_g(*P.cycle(5), [0, 0, 1, 1, 0]),
+                                 P.to_g(*P.star(5), [1, 0, 0, 1, 2])]}
+    for (name, labeled), texts in cases.items():
+        hg = host_graph(name, labeled)
+        rg, _ = pm.reorder_by_degree(hg)
+        g0 = pm.GraphPreprocessor.from_host(hg, labeled=labeled)
+        g1 = pm.GraphPreprocessor.from_host(rg, labeled=labeled)
+        try:
+            for text in texts:
+                p = pm.PatternPreprocessor(text=text, labeled=labeled)
+                want, _ = oracle_count(hg, text, labeled)
+                a, _ = ctx.match(g0, [p])
+                b, _ = ctx.match(g1, [p])
+                assert a[0] == want and b[0] == want, (name, text)
+        finally:
+            g0.close()
+            g1.close()
