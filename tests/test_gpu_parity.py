@@ -323,3 +323,24 @@ def test_gpu_degree_order_keeps_counts(ctx):
         finally:
             g0.close()
             g1.close()
+
+
+def test_gpu_deadline_returns_timeout_and_context_stays_usable(ctx):
+    """A launch that runs past its deadline stops on its own (every wait and
+    every warp checks the clock), reports PM_ERR_TIMEOUT, and leaves the
+    context usable: the next launch gives the full count."""
+    from pumatch_b200 import patterns as P
+    hg = pm.gen_chung_lu(20000, 200000, gamma=2.1, i0=5.0, max_w=2000.0, seed=7)
+    g = pm.GraphPreprocessor.from_host(hg)
+    try:
+        p = pm.PatternPreprocessor(text=P.to_g(*P.clique(6)), labeled=False)
+        full, st = ctx.match(g, [p])
+        if st["kernel_ms"] < 20:
+            pytest.skip(f"the launch takes {st['kernel_ms']:.1f} ms: too quick to cut short")
+        with pytest.raises(pm.PmError) as e:
+            ctx.match(g, [p], timeout_ms=1)
+        assert e.value.status == pm.PM_ERR_TIMEOUT
+        again, st2 = ctx.match(g, [p])
+        assert again == full and st2["device_status"] == 0
+    finally:
+        g.close()
