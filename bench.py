@@ -35,8 +35,8 @@ sys.path.insert(0, ROOT)
 import pumatch_b200 as pm  # noqa: E402
 from pumatch_b200 import patterns as P  # noqa: E402
 
-# name -> definition.  Graph sizes/seeds follow the configuration each one
-# stands in for; the reasons for each stand-in are in DESIGN.md.
+# name -> definition.  Each keeps the graph family, sizes and seeds of the
+# configuration it stands in for, with a query that finishes exactly.
 _CL100K = dict(kind="chung_lu", n=100_000, m=1_000_000, gamma=2.1, i0=10.0, max_w=5000.0, seed=1)
 _RMAT1M = dict(kind="rmat", n=1 << 20, m=16 << 20, a=0.57, b=0.19, c=0.19, seed=2)
 _RMAT128K = dict(kind="rmat", n=1 << 17, m=16 << 17, a=0.57, b=0.19, c=0.19, seed=2)

@@ -10,7 +10,8 @@ a count:
   * page residency (paged graphs): pages are scored by the predicted reads of
     the roots whose first two vertices' lists live in them, and the frame pool
     starts with the highest-scoring pages instead of the first ones.
-The plain path is the fallback (no model) and the judge of prediction error.
+The plain path is the fallback (no model) and the baseline that prediction
+error and speed are measured against.
 """
 from __future__ import annotations
 

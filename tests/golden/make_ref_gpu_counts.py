@@ -7,7 +7,7 @@ LABELED / GRAPH_DEGREE selected by -include shims, device code built with -G
 as the reference's Makefile does).  Reads only files under
 this repository.
 
-    python tests/golden/make_ref_gpu_counts.py --out gpurun_out/ref_gpu_counts.json
+    python tests/golden/make_ref_gpu_counts.py --out ref_gpu_counts.json
 
 Each record: graph, pattern, labeled, truncate (the binary's GRAPH_DEGREE),
 count (last stdout line of the binary), ms.  Unlabeled patterns whose last
