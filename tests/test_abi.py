@@ -123,3 +123,60 @@ def test_run_option_keywords():
     assert o.lane_subtree_max == -1
     with pytest.raises(TypeError):
         pm.Context._opts(leaf_mode=1)
+
+
+def test_new_fields_match_c():
+    src = r'''
+#include <stdio.h>
+#include <stddef.h>
+#include "pumatch.h"
+int main(void){
+ printf("%zu %zu %zu %zu %zu %zu\n", offsetof(pm_graph_opts, static_pool_bytes), offsetof(pm_graph_info, n_static_frames),
+        offsetof(pm_run_opts, leaf_per_lane), offsetof(pm_run_opts, lane_subtree_max), offsetof(pm_stats, warp_ns),
+        offsetof(pm_stats, idle_ns));
+ return 0; }'''
+    import ctypes as C
+    import tempfile
+    d = tempfile.mkdtemp()
+    open(os.path.join(d, "p.c"), "w").write(src)
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), "-o", os.path.join(d, "p"), os.path.join(d, "p.c")],
+                   check=True)
+    vals = [int(x) for x in subprocess.run([os.path.join(d, "p")], capture_output=True, text=True).stdout.split()]
+    assert vals == [pm.GraphOpts.static_pool_bytes.offset, pm.GraphInfo.n_static_frames.offset,
+                    pm.RunOpts.leaf_per_lane.offset, pm.RunOpts.lane_subtree_max.offset, pm.Stats.warp_ns.offset,
+                    pm.Stats.idle_ns.offset]
+
+
+def test_c_program_links_and_runs_host_entry_points(tmp_path):
+    """A plain C caller, as INTEGRATION.md's snippet: compile a pattern,
+    describe it, build and renumber a graph, and get PM_ERR_NO_DEVICE (not a
+    CPU fallback) from the device entry points."""
+    src = r'''
+#include <stdio.h>
+#include <stdlib.h>
+#include "pumatch.h"
+int main(void){
+  pm_plan* p = NULL;
+  const char* k4 = "v 0 1\nv 1 1\nv 2 1\nv 3 1\ne 0 1 1\ne 0 2 1\ne 0 3 1\ne 1 2 1\ne 1 3 1\ne 2 3 1\n";
+  if (pm_plan_compile_text(k4, 0, &p) != PM_OK) { printf("compile %s\n", pm_last_error()); return 1; }
+  pm_plan_desc d;
+  if (pm_plan_describe(p, &d) != PM_OK) return 2;
+  uint64_t* rp = NULL; int32_t* ci = NULL; int64_t nadj = 0; int32_t md = 0;
+  if (pm_gen_chung_lu(500, 2000, 2.1, 5.0, 100.0, 3, &rp, &ci, &nadj, &md) != PM_OK) return 3;
+  uint64_t* rp2 = malloc(sizeof(uint64_t) * 501); int32_t* ci2 = malloc(sizeof(int32_t) * nadj);
+  if (pm_reorder_by_degree(500, nadj, rp, ci, NULL, rp2, ci2, NULL, NULL) != PM_OK) return 4;
+  pm_ctx* c = NULL;
+  pm_status s = pm_ctx_create(0, &c);
+  printf("%d %d %d %lld %d\n", d.nnodes, d.multiplicity, (int)(rp2[1] - rp2[0]) == md, (long long)nadj,
+         s == PM_ERR_NO_DEVICE);
+  pm_host_free(rp); pm_host_free(ci); free(rp2); free(ci2); pm_plan_free(p);
+  return 0; }'''
+    lib_dir = os.path.dirname(pm.LIB_PATH)
+    exe = str(tmp_path / "c_caller")
+    open(str(tmp_path / "c.c"), "w").write(src)
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), "-o", exe, str(tmp_path / "c.c"), "-L", lib_dir,
+                    "-lpumatch_b200", "-Wl,-rpath," + lib_dir], check=True)
+    r = subprocess.run([exe], capture_output=True, text=True)
+    assert r.returncode == 0, r.stdout + r.stderr
+    nn, mult, maxfirst, nadj, nodev = r.stdout.split()
+    assert (nn, mult, maxfirst, nodev) == ("4", "24", "1", "1") and int(nadj) == 4000
