@@ -151,3 +151,26 @@ def test_cli_order_and_halve_match_the_reference_tools(tmp_path, name):
         ma = open(ours + suffix + ".meta.txt").read().split()
         mb = open(theirs + suffix + ".meta.txt").read().split()
         assert [int(x) for x in ma] == [int(x) for x in mb], (name, flag)
+
+
+def test_cli_transform_errors(tmp_path):
+    cli = os.path.join(os.path.dirname(pm.CLI_PATH), "convert")
+    r = subprocess.run([cli, "--halve", str(tmp_path / "missing")], capture_output=True, text=True)
+    assert r.returncode == 1 and "read" in r.stderr
+    r = subprocess.run([cli, "--order=degree"], capture_output=True, text=True)
+    assert r.returncode == 2
+    r = subprocess.run([cli], capture_output=True, text=True)
+    assert r.returncode == 2 and "--order=degree" in r.stderr and "--halve" in r.stderr
+
+
+def test_cli_order_keeps_labels(tmp_path):
+    """`convert --order=degree` on a labeled graph writes the labels in the
+    new vertex order."""
+    cli = os.path.join(os.path.dirname(pm.CLI_PATH), "convert")
+    pre = str(tmp_path / "g")
+    hg = _copy_graph("rmat512", pre, labeled=True)
+    r = subprocess.run([cli, "--order=degree", pre], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    og = pm.HostGraph.read(pre + ".ord", labeled=True)
+    rg, nid = pm.reorder_by_degree(hg)
+    assert (og.rowptr == rg.rowptr).all() and (og.colidx == rg.colidx).all() and (og.labels == rg.labels).all()
