@@ -376,6 +376,15 @@ pm_status pm_match_static(const uint64_t* d_rowptr, const int32_t* d_colidx, con
                           const pm_run_opts* opts, void* stream, uint64_t* count_out,
                           pm_stats* stats_out);
 
+/* The JSON sidecar of one launch (the reference prints only "ms count";
+ * its counters g_total_cpu_m / g_total_cpu_bytes, src/buffer.cu:11-19, are
+ * never printed): per-pattern counts, kernel ms, matches/s, set operations,
+ * algorithmic bytes and GB/s, page traffic, warp idle share.  Writes at most
+ * cap bytes (NUL-terminated) into buf; *len_out (optional) receives the
+ * length the whole document needs.  PM_ERR_INVALID when it does not fit. */
+pm_status pm_stats_json(const pm_stats* stats, const uint64_t* counts, int n_counts, char* buf, size_t cap,
+                        size_t* len_out);
+
 const char* pm_strerror(pm_status s);
 const char* pm_last_error(void);
 

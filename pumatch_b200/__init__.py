@@ -101,6 +101,7 @@ SIGNATURES = {
     "pm_convert_snap": (C.c_int, [C.c_char_p, C.c_char_p, C.c_int, C.c_int, C.POINTER(C.c_int64),
                                   C.POINTER(C.c_int64)]),
     "pm_reorder_by_degree": (C.c_int, [C.c_int64, C.c_int64, _P, _P, _P, _P, _P, _P, _P]),
+    "pm_stats_json": (C.c_int, [_P, _P, C.c_int, C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)]),
     "pm_halve": (C.c_int, [C.c_int64, C.c_int64, _P, _P, _P, _P, C.POINTER(C.c_int64), C.POINTER(C.c_int32)]),
     "pm_gen_chung_lu": (C.c_int, [C.c_int64, C.c_int64, C.c_double, C.c_double, C.c_double, C.c_uint64,
                                   _PP, _PP, C.POINTER(C.c_int64), C.POINTER(C.c_int32)]),

@@ -3,6 +3,7 @@
 //   test <graph-prefix> <pattern.g> [--labeled=0|1] [--truncate=N] [--device=D]
 //        [--paged] [--frame-mb=M] [--static-mb=S] [--page-kb=K] [--batch=<list file>]
 //        [--warps=W] [--chunk=C] [--split=S] [--tuned=<autotuner json>]
+//        [--json=<path>]
 //
 // Same positional arguments and output as the reference's driver
 // (test.cu:15-21, 200-209): the last stdout line is "<kernel ms> <count>" and
@@ -13,6 +14,7 @@
 // With --batch, <pattern.g> is ignored and each line of the list file names a
 // pattern; all run in one launch and one "<ms> <count>" line is printed per
 // pattern in list order (ms is the shared launch time).
+// --json writes the launch's statistics (pm_stats_json) to <path>.
 // --tuned reads the "best" record the autotuner writes (warps_per_block,
 // chunk, split_level1, page_kb); explicit flags after it override it.
 #include <cstdio>
@@ -53,7 +55,7 @@ int main(int argc, char** argv) {
   if (argc < 3) {
     fprintf(stderr, "usage: test <graph-prefix> <pattern.g> [--labeled=0|1] [--truncate=N] [--device=D]\n"
                     "            [--paged] [--frame-mb=M] [--static-mb=S] [--page-kb=K] [--batch=<list>]\n"
-                    "            [--warps=W] [--chunk=C] [--split=S] [--tuned=<json>]\n");
+                    "            [--warps=W] [--chunk=C] [--split=S] [--tuned=<json>] [--json=<path>]\n");
     return 2;
   }
   const char* prefix = argv[1];
@@ -61,7 +63,7 @@ int main(int argc, char** argv) {
   int labeled = 1, truncate = 0, device = 0, paged = 0;
   long long frame_mb = 4096, static_mb = 0, page_kb = 64;
   long long warps = 0, chunk = 0, split = 0;
-  std::string batch;
+  std::string batch, json_path;
   for (int i = 3; i < argc; i++) {
     const char* a = argv[i];
     if (!strncmp(a, "--tuned=", 8)) {
@@ -75,6 +77,7 @@ int main(int argc, char** argv) {
       if (tuned_int(text, "split_level1", &v)) split = v;
       if (tuned_int(text, "page_kb", &v)) page_kb = v;
     }
+    else if (!strncmp(a, "--json=", 7)) json_path = a + 7;
     else if (!strncmp(a, "--warps=", 8)) warps = atoll(a + 8);
     else if (!strncmp(a, "--chunk=", 8)) chunk = atoll(a + 8);
     else if (!strncmp(a, "--split=", 8)) split = atoll(a + 8);
@@ -140,6 +143,19 @@ int main(int argc, char** argv) {
   fprintf(stderr, "roots %llu, set ops %llu, algorithmic bytes %llu, root filter %.3f ms\n",
           (unsigned long long)st.n_roots, (unsigned long long)st.set_ops,
           (unsigned long long)st.alg_bytes, st.roots_ms);
+  if (!json_path.empty()) {
+    size_t need = 0;
+    pm_stats_json(&st, counts.data(), (int)counts.size(), nullptr, 0, &need);
+    std::vector<char> doc(need);
+    FILE* jf = fopen(json_path.c_str(), "w");
+    if (!jf || pm_stats_json(&st, counts.data(), (int)counts.size(), doc.data(), doc.size(), nullptr) != PM_OK) {
+      fprintf(stderr, "test: cannot write %s\n", json_path.c_str());
+      if (jf) fclose(jf);
+      return 1;
+    }
+    fprintf(jf, "%s\n", doc.data());
+    fclose(jf);
+  }
   const float ms = st.kernel_ms;
   for (size_t i = 0; i < plans.size(); i++) {
     std::cout << ms << ' ' << (unsigned long long)counts[i] << std::endl;

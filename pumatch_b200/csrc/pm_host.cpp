@@ -349,6 +349,39 @@ using namespace pm;
 
 extern "C" const char* pm_last_error(void) { return g_last_error.c_str(); }
 
+extern "C" pm_status pm_stats_json(const pm_stats* st, const uint64_t* counts, int n_counts, char* buf,
+                                   size_t cap, size_t* len_out) {
+  if (!st || (n_counts > 0 && !counts) || n_counts < 0 || (cap > 0 && !buf))
+    return fail(PM_ERR_INVALID, "pm_stats_json: bad arguments");
+  std::string j = "{\"counts\": [";
+  uint64_t total = 0;
+  for (int i = 0; i < n_counts; i++) {
+    j += (i ? ", " : "") + std::to_string((unsigned long long)counts[i]);
+    total += counts[i];
+  }
+  const double s = st->kernel_ms / 1000.0;
+  char tmp[768];
+  snprintf(tmp, sizeof(tmp),
+           "], \"kernel_ms\": %.3f, \"roots_ms\": %.3f, \"matches_per_s\": %.6g, \"n_roots\": %llu, "
+           "\"set_ops\": %llu, \"alg_bytes\": %llu, \"alg_gbs\": %.6g, \"splits\": %llu, "
+           "\"page_hits\": %llu, \"page_misses\": %llu, \"pages_loaded\": %llu, \"h2d_page_bytes\": %llu, "
+           "\"zero_copy_bytes\": %llu, \"evictions\": %llu, \"warp_idle_share\": %.4f, "
+           "\"grid_blocks\": %d, \"block_threads\": %d, \"device_status\": %u}",
+           st->kernel_ms, st->roots_ms, s > 0 ? (double)total / s : 0.0, (unsigned long long)st->n_roots,
+           (unsigned long long)st->set_ops, (unsigned long long)st->alg_bytes,
+           s > 0 ? (double)st->alg_bytes / s / 1e9 : 0.0, (unsigned long long)st->splits,
+           (unsigned long long)st->page_hits, (unsigned long long)st->page_misses,
+           (unsigned long long)st->pages_loaded, (unsigned long long)st->h2d_page_bytes,
+           (unsigned long long)st->zero_copy_bytes, (unsigned long long)st->evictions,
+           st->warp_ns ? (double)st->idle_ns / (double)st->warp_ns : 0.0, st->grid_blocks, st->block_threads,
+           st->device_status);
+  j += tmp;
+  if (len_out) *len_out = j.size() + 1;
+  if (j.size() + 1 > cap) return fail(PM_ERR_INVALID, "pm_stats_json: needs %zu bytes", j.size() + 1);
+  memcpy(buf, j.c_str(), j.size() + 1);
+  return PM_OK;
+}
+
 extern "C" const char* pm_strerror(pm_status s) {
   switch (s) {
     case PM_OK: return "ok";

@@ -180,3 +180,21 @@ int main(void){
     assert r.returncode == 0, r.stdout + r.stderr
     nn, mult, maxfirst, nadj, nodev = r.stdout.split()
     assert (nn, mult, maxfirst, nodev) == ("4", "24", "1", "1") and int(nadj) == 4000
+
+
+def test_stats_json_sidecar():
+    import ctypes as C
+    import json as js
+    st = pm.Stats()
+    st.kernel_ms, st.n_roots, st.set_ops, st.alg_bytes = 2000.0, 7, 11, 4_000_000_000
+    st.page_hits, st.warp_ns, st.idle_ns, st.grid_blocks = 5, 1000, 250, 444
+    counts = (C.c_uint64 * 2)(10, 2**63)
+    need = C.c_size_t()
+    assert pm.lib().pm_stats_json(C.byref(st), counts, 2, None, 0, C.byref(need)) == pm.PM_ERR_INVALID
+    buf = C.create_string_buffer(need.value)
+    assert pm.lib().pm_stats_json(C.byref(st), counts, 2, buf, need.value, None) == pm.PM_OK
+    d = js.loads(buf.value.decode())
+    assert d["counts"] == [10, 2**63] and d["set_ops"] == 11 and d["n_roots"] == 7
+    assert abs(d["alg_gbs"] - 2.0) < 1e-9 and abs(d["warp_idle_share"] - 0.25) < 1e-9
+    assert abs(d["matches_per_s"] - (10 + 2**63) / 2.0) / d["matches_per_s"] < 1e-6
+    assert d["grid_blocks"] == 444 and d["device_status"] == 0

@@ -249,6 +249,13 @@ def test_gpu_cli_output(tmp_path):
     assert int(count) == want
     rec = (tmp_path / "result.txt").read_text().strip().split("\t")
     assert rec[0] == prefix and rec[1] == str(pat) and int(rec[3]) == want
+    # the JSON sidecar carries the same count and the launch's counters
+    side = tmp_path / "stats.json"
+    r = subprocess.run([pm.CLI_PATH, prefix, str(pat), "--json=" + str(side)], capture_output=True, text=True,
+                       cwd=tmp_path)
+    assert r.returncode == 0, r.stderr
+    d = json.loads(side.read_text())
+    assert d["counts"] == [want] and d["set_ops"] > 0 and d["device_status"] == 0
     r = subprocess.run([pm.CLI_PATH, prefix, str(pat), "--labeled=0", "--truncate=8"], capture_output=True,
                        text=True, cwd=tmp_path)
     assert r.returncode == 0, r.stderr
