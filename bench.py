@@ -3,18 +3,29 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME] [--impl ours|reference]
 
-A step is one full query: the GPU root filter plus the persistent DFS launch
-over every root edge of the workload's graph, counts read back.  `value` is
-matches/s with the graph already resident in HBM (device time, CUDA events on
-the library's own stream, max over ranks); `e2e` is the same metric through the
-public API with host buffers (graph upload + match + count read-back inside the
-timed region).  With N>1 ranks the query's root chunks are sharded across ranks
-(rank r takes chunks r, r+N, ...) and the counts are summed with one 8-byte
-all-reduce per pattern.
+A step is one query over the workload's root edges: the GPU root filter plus
+the persistent DFS launch, counts read back.  The default workload is the
+configured small query -- the 7-cycle, unlabeled, on the Chung-Lu graph of
+100K vertices and 1M edges -- whose full root list is out of reach of any
+exact enumerator (about 1.4e16 set operations), so a step runs a seeded
+sample of its root edges (tests/golden/root_samples.json states the rule);
+every sampled root's count is checked against the oracle's exact per-root
+count in that fixture, and the run fails on any difference.  Workloads
+without a sample run every root edge and are checked per root on the roots
+the CPU baseline samples.
+
+`value` is matches/s with the graph already resident in HBM (device time,
+CUDA events on the library's own stream, max over ranks); `e2e` is the same
+metric through the public API with host buffers (graph upload + match +
+count read-back inside the timed region).  With N>1 ranks the root chunks are
+sharded across ranks (rank r takes chunks r, r+N, ...) and the counts are
+summed with one 8-byte all-reduce per pattern.
 
 --impl reference times the CPU implementation of the same path (the oracle
-port; the reference itself has no CPU implementation of its matcher) on the
-host cores, one bounded root sample per step, rank 0 only.
+port; the reference itself has no CPU implementation of its matcher) on all
+host cores, one bounded sample of the same roots per step, rank 0 only; it
+builds its inputs with the oracle's generators and never loads the product
+library.
 """
 from __future__ import annotations
 
@@ -36,13 +47,21 @@ import pumatch_b200 as pm  # noqa: E402
 from pumatch_b200 import patterns as P  # noqa: E402
 
 # name -> definition.  Each keeps the graph family, sizes and seeds of the
-# configuration it stands in for, with a query that finishes exactly.
+# configuration it stands in for.  A workload with a "sample" runs the seeded
+# root sample of that name in tests/golden/root_samples.json.
 _CL100K = dict(kind="chung_lu", n=100_000, m=1_000_000, gamma=2.1, i0=10.0, max_w=5000.0, seed=1)
 _RMAT1M = dict(kind="rmat", n=1 << 20, m=16 << 20, a=0.57, b=0.19, c=0.19, seed=2)
 _RMAT128K = dict(kind="rmat", n=1 << 17, m=16 << 17, a=0.57, b=0.19, c=0.19, seed=2)
 WORKLOADS = {
-    # Chung-Lu 100K vertices / 1M edges, gamma 2.1, expected degrees capped
-    # at 5,000, unlabeled, in HBM; one 7-vertex query: the 7-clique.
+    # the configured small query: Chung-Lu 100K vertices / 1M edges, gamma
+    # 2.1, expected degrees capped at 5,000, unlabeled, in HBM; the 7-cycle,
+    # on a seeded sample of its root edges
+    "chunglu100k_c7": dict(graph=_CL100K, labeled=False, n_labels=0, patterns=[("C7", P.cycle(7))],
+                           sample="chunglu100k_c7"),
+    # the same query over its whole root list: only for --root-begin/--root-limit
+    # slices (profiling); the whole list is out of reach
+    "chunglu100k_c7_all": dict(graph=_CL100K, labeled=False, n_labels=0, patterns=[("C7", P.cycle(7))]),
+    # the same graph, every root edge of the 7-clique
     "chunglu100k_k7": dict(graph=_CL100K, labeled=False, n_labels=0, patterns=[("K7", P.clique(7))]),
     # the same graph with 16 uniform labels and the 7-cycle (labeled semantics)
     "chunglu100k_c7_lab16": dict(graph=_CL100K, labeled=True, n_labels=16, label_seed=102, pattern_label_seed=202,
@@ -67,22 +86,41 @@ WORKLOADS = {
                                       pattern_label_seed=202, patterns=[("C5t2", P.cycle_tail(5, 2))],
                                       paged=dict(frame_fraction=0.88, static_fraction=0.6, page_bytes=16 << 10)),
 }
-DEFAULT_WORKLOAD = "chunglu100k_k7"
+DEFAULT_WORKLOAD = "chunglu100k_c7"
+SAMPLES_PATH = os.path.join(ROOT, "tests", "golden", "root_samples.json")
 
 
-def make_graph(g, seed=None):
+def _oracle():
+    """The CPU oracle (test infrastructure): the checker and the CPU arm."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pm_oracle as orc
+    return orc
+
+
+def make_graph(g, seed=None, via_oracle=False):
+    """Host CSR of a workload graph: the product's generator, or (for the CPU
+    arm, which must not load the product library) the oracle's restatement of
+    it, which a CPU test pins to the same arrays."""
     seed = g["seed"] if seed is None else seed
+    if via_oracle:
+        orc = _oracle()
+        if g["kind"] == "chung_lu":
+            rp, ci = orc.gen_chung_lu(g["n"], g["m"], g["gamma"], g["i0"], g["max_w"], seed)
+        else:
+            rp, ci = orc.gen_rmat(g["n"], g["m"], g["a"], g["b"], g["c"], seed)
+        return pm.HostGraph(rp, ci)
     if g["kind"] == "chung_lu":
         return pm.gen_chung_lu(g["n"], g["m"], gamma=g["gamma"], i0=g["i0"], max_w=g["max_w"], seed=seed)
     return pm.gen_rmat(g["n"], g["m"], a=g["a"], b=g["b"], c=g["c"], seed=seed)
 
 
-def build_workload(name, graph_seed=None):
+def build_workload(name, graph_seed=None, via_oracle=False):
     w = WORKLOADS[name]
-    hg = make_graph(w["graph"], graph_seed)
+    hg = make_graph(w["graph"], graph_seed, via_oracle)
     if w["labeled"]:
         ls = w["label_seed"] if graph_seed is None else w["label_seed"] + 1000 * graph_seed
-        hg = pm.HostGraph(hg.rowptr, hg.colidx, pm.gen_labels(hg.n, w["n_labels"], seed=ls))
+        labels = _oracle().gen_labels(hg.n, w["n_labels"], ls) if via_oracle else pm.gen_labels(hg.n, w["n_labels"], ls)
+        hg = pm.HostGraph(hg.rowptr, hg.colidx, labels)
     if "batch_seed" in w:
         texts = P.batch_of_20(seed=w["batch_seed"], n_labels=w["n_labels"])
     else:
@@ -91,6 +129,32 @@ def build_workload(name, graph_seed=None):
             labs = P.seeded_labels(k, w["n_labels"], w["pattern_label_seed"] + i) if w["labeled"] else None
             texts.append((pname, P.to_g(k, edges, labs)))
     return w, hg, texts
+
+
+def load_sample(w, hg):
+    """The workload's root sample record, after checking that this graph is
+    the one the sample was drawn on (arrays' sha256)."""
+    if "sample" not in w:
+        return None
+    import hashlib
+    with open(SAMPLES_PATH) as f:
+        rec = json.load(f)[w["sample"]]
+    h = hashlib.sha256()
+    h.update(hg.rowptr.tobytes())
+    h.update(hg.colidx.tobytes())
+    if h.hexdigest() != rec["graph_sha256"]:
+        raise SystemExit(f"the generated graph differs from the one {w['sample']} was drawn on")
+    return rec
+
+
+def sample_config(rec):
+    if rec is None:
+        return None
+    k = len(rec["roots"])
+    return {"rule": rec["rule"], "roots": k, "of": rec["n_roots_total"],
+            "root_ids": [r["index"] for r in rec["roots"]], "set_ops": rec["set_ops"],
+            "query_set_ops_estimate": rec["query_set_ops_estimate"],
+            "share_of_query": rec["set_ops"] / rec["query_set_ops_estimate"]}
 
 
 def place_graph(w, hg, device):
@@ -186,14 +250,30 @@ def profile_traffic(workload):
         return None
 
 
-def cpu_sample_run(hg, texts, labeled, threads, target_s=15.0, seed=5, max_frac=1.0):
-    """Times the oracle on a seeded random root sample sized for ~target_s.
-    Returns (matches, seconds, roots_in_sample, roots_total)."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import pm_oracle as orc
+def cpu_measure(hg, texts, labeled, threads, sample=None, time_limit_s=15.0, seed=5, per_root=False):
+    """Times the oracle on the host cores.
+
+    With a root sample: the sampled roots' DFS pieces (level-1 candidates) in
+    a seeded shuffled order, stopped at time_limit_s; the rate is matches per
+    second over the pieces done.  Without one: seeded random root samples,
+    grown until a run takes about a quarter of time_limit_s; with per_root the
+    per-root counts of the last sample are returned for the parity check.
+    Returns dict(matches, seconds, sample text[, roots, per_root])."""
+    orc = _oracle()
     g = orc.Graph(hg.rowptr, hg.colidx, hg.labels if labeled else None)
+    plans = [orc.plan(t, labeled) for _, t in texts]
+    mult = [1 if labeled else p.multiplicity for p in plans]
+    if sample is not None:
+        p = plans[0]
+        rts = orc.roots(g, p)[[r["index"] for r in sample["roots"]]]
+        t0 = time.perf_counter()
+        c, _, done, tot, _ = orc.count_split(g, p, rts, threads=threads, time_limit_s=time_limit_s,
+                                             shuffle_seed=seed)
+        dt = time.perf_counter() - t0
+        return {"matches": c * mult[0], "seconds": dt,
+                "sample": f"{done} of the {tot} level-1 pieces of the {len(rts)} sampled root edges (seeded "
+                          f"shuffled order), {dt:.1f} s on {threads} threads"}
     rng = np.random.default_rng(seed)
-    plans = [(orc.plan(t, labeled)) for _, t in texts]
     roots = [orc.roots(g, p) for p in plans]
     total_roots = sum(len(r) for r in roots)
     frac = 1e-4
@@ -202,44 +282,53 @@ def cpu_sample_run(hg, texts, labeled, threads, target_s=15.0, seed=5, max_frac=
         for r in roots:
             k = max(1, int(len(r) * frac))
             idx = np.sort(rng.choice(len(r), size=min(k, len(r)), replace=False))
-            samples.append(np.ascontiguousarray(r[idx]))
+            samples.append(idx)
         t0 = time.perf_counter()
-        m = 0
-        for p, s in zip(plans, samples):
-            c, _ = orc.count(g, p, s, threads=threads)
-            m += c if labeled else c * p.multiplicity
+        m, per = 0, []
+        for p, r, idx, mu in zip(plans, roots, samples, mult):
+            c, pr, _, _, _ = orc.count_split(g, p, r[idx], threads=threads)
+            m += c * mu
+            per.append(pr)
         dt = time.perf_counter() - t0
         n_s = sum(len(s) for s in samples)
-        if dt >= target_s / 4 or frac >= max_frac:
-            return m, dt, n_s, total_roots
-        frac = min(max_frac, frac * max(2.0, min(50.0, (target_s / 2) / max(dt, 1e-3))))
+        if dt >= time_limit_s / 4 or frac >= 1.0:
+            out = {"matches": m, "seconds": dt,
+                   "sample": f"{n_s} of {total_roots} root edges, seeded random sample, {dt:.1f} s of oracle DFS"}
+            if per_root:
+                out["roots"] = samples
+                out["per_root"] = per
+            return out
+        frac = min(1.0, frac * max(2.0, min(50.0, (time_limit_s / 2) / max(dt, 1e-3))))
 
 
 def run_reference(args, workload):
-    """CPU arm: the oracle port of the path, all host threads, bounded samples."""
+    """CPU arm: the oracle port of the path, all host threads, a bounded
+    sample of the same workload per step.  Inputs come from the oracle's own
+    generators; the product library is never loaded."""
     rank, world, _ = dist_env()
     if rank != 0:
         return
-    w, hg, texts = build_workload(workload)
+    w, hg, texts = build_workload(workload, via_oracle=True)
+    sample = load_sample(w, hg)
     threads = os.cpu_count() or 1
-    for _ in range(args.warmup):
-        cpu_sample_run(hg, texts, w["labeled"], threads, target_s=2.0, seed=99)
-    tot_m, tot_s, tot_n = 0, 0.0, 0
-    total_roots = 0
+    for k in range(args.warmup):
+        cpu_measure(hg, texts, w["labeled"], threads, sample, time_limit_s=2.0, seed=99 + k)
+    tot_m, tot_s, descr = 0, 0.0, ""
     for k in range(args.steps):
-        m, dt, n_s, total_roots = cpu_sample_run(hg, texts, w["labeled"], threads, target_s=10.0, seed=k + 1)
-        tot_m += m
-        tot_s += dt
-        tot_n += n_s
+        r = cpu_measure(hg, texts, w["labeled"], threads, sample, time_limit_s=10.0, seed=k + 1)
+        tot_m += r["matches"]
+        tot_s += r["seconds"]
+        descr = r["sample"]
     value = tot_m / tot_s if tot_s > 0 else 0.0
-    sample = f"{tot_n} of {total_roots} root edges per {args.steps} steps (seeded random samples)"
+    sample_txt = f"{args.steps} steps, each {descr}"
     line = {
         "impl": "reference", "metric": "matches_per_s", "value": value, "unit": "matches/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * tot_s / max(args.steps, 1),
         "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
         "config": {"workload": workload, "graph": w["graph"], "labeled": w["labeled"],
-                   "patterns": [p for p, _ in texts], "sample": sample},
-        "cpu_baseline": {"value": value, "unit": "matches/s", "cores": threads, "kind": "port", "sample": sample},
+                   "patterns": [p for p, _ in texts], "root_sample": sample_config(sample)},
+        "cpu_baseline": {"value": value, "unit": "matches/s", "cores": threads, "kind": "port",
+                         "sample": sample_txt},
         "e2e": {"value": value, "unit": "matches/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -257,6 +346,7 @@ def run_ours(args, workload):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local))
     w, hg, texts = build_workload(workload)
+    sample = load_sample(w, hg)
     labeled = w["labeled"]
     plans = [pm.PatternPreprocessor(text=t, labeled=labeled) for _, t in texts]
     ctx = pm.Context(local)
@@ -268,10 +358,28 @@ def run_ours(args, workload):
                   leaf_per_lane=int(args.leaf_per_lane), lane_subtree_max=args.lane_subtree_max, **shard)
     if args.root_limit > 0:
         run_kw.update(root_begin=args.root_begin, root_end=args.root_begin + args.root_limit)
+    # per-root counts of plan 0, for the parity check
+    n_roots = ctx.count_roots(graph, plans[0])
+    root_counts = torch.zeros(max(n_roots, 1), dtype=torch.int64, device="cuda")
+    run_kw["root_counts_ptr"] = root_counts.data_ptr()
+    order_h = None
+    if sample is not None:
+        if len(plans) != 1 or args.root_limit > 0:
+            raise SystemExit("a sampled workload runs one pattern over its sample")
+        roots_all = ctx.roots(graph, plans[0])
+        if len(roots_all) != sample["n_roots_total"]:
+            raise SystemExit("root list length differs from the sample's")
+        for r in sample["roots"]:
+            if tuple(roots_all[r["index"]]) != (r["v0"], r["v1"]):
+                raise SystemExit(f"root {r['index']} is not the sampled edge")
+        order_h = torch.tensor([r["index"] for r in sample["roots"]], dtype=torch.int32).pin_memory()
+        order = order_h.to("cuda")
+        run_kw.update(root_order_ptr=order.data_ptr(), root_begin=0, root_end=len(order_h))
 
     def one_step():
-        counts, st = ctx.match(graph, plans, **run_kw)
-        return counts, st
+        with torch.cuda.stream(stream):
+            root_counts.zero_()
+        return ctx.match(graph, plans, **run_kw)
 
     def reduce_counts(counts):
         if dist is None:
@@ -314,18 +422,30 @@ def run_ours(args, workload):
         total_ms = float(t[0])
     matches_per_step = sum(counts_total)
     value = matches_per_step * args.steps / (total_ms / 1000.0)
+    per_root_gpu = root_counts.cpu().numpy()
+    if dist:
+        t = root_counts.clone()
+        dist.all_reduce(t)
+        per_root_gpu = t.cpu().numpy()
 
     # end to end through the public API with host buffers
     e2e_ms = []
     h2d = hg.rowptr.nbytes + hg.colidx.nbytes + (hg.labels.nbytes if labeled else 0)
     d2h = 8 * len(plans)
+    if order_h is not None:
+        h2d += order_h.numel() * 4
     for k in range(max(1, min(args.steps, 3))):
         torch.cuda.synchronize()
         if dist:
             dist.barrier()
         t0 = time.perf_counter()
         g2 = place_graph(w, hg, local)
-        c2, _ = ctx.match(g2, plans, **run_kw)
+        kw2 = dict(run_kw)
+        kw2.pop("root_counts_ptr")
+        if order_h is not None:
+            o2 = order_h.to("cuda", non_blocking=True)
+            kw2["root_order_ptr"] = o2.data_ptr()
+        c2, _ = ctx.match(g2, plans, **kw2)
         g2.close()
         torch.cuda.synchronize()
         dt = (time.perf_counter() - t0) * 1000.0
@@ -345,6 +465,20 @@ def run_ours(args, workload):
         per_launch_s = (sum(kern_ms) / args.steps) / 1000.0
         achieved = per_launch_bytes / per_launch_s / 1e9 if per_launch_s > 0 else 0.0
         traffic = profile_traffic(workload)
+        parity = None
+        ok = True
+        mult = 1 if labeled else plans[0].PatternMultiplicity
+        if sample is not None:
+            # every sampled root against the oracle's exact per-root count
+            bad = [r["index"] for r in sample["roots"] if int(per_root_gpu[r["index"]]) != r["raw_count"]]
+            ok = (not bad and counts_total[0] == sample["count"] and set_ops // args.steps == sample["set_ops"]
+                  and alg_bytes // args.steps == sample["alg_bytes"])
+            parity = {"roots_checked": len(sample["roots"]), "ok": ok, "mismatched_roots": bad,
+                      "count": counts_total[0], "oracle_count": sample["count"],
+                      "set_ops_equal": set_ops // args.steps == sample["set_ops"],
+                      "alg_bytes_equal": alg_bytes // args.steps == sample["alg_bytes"],
+                      "against": "oracle exact per-root counts, set operations and algorithmic bytes "
+                                 "(tests/golden/root_samples.json)"}
         line = {
             "metric": "matches_per_s", "value": value, "unit": "matches/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
@@ -352,6 +486,7 @@ def run_ours(args, workload):
             "data": "synthetic",
             "config": {"workload": workload, "graph": w["graph"], "labeled": w["labeled"],
                        "patterns": [p for p, _ in texts], "counts": counts_total,
+                       "root_sample": sample_config(sample),
                        "kernel_variant": ["default", "regs64", "regs85", "uncapped"][args.high_occupancy] +
                                          ("+leaf_per_lane" if args.leaf_per_lane else "") +
                                          (f"+lane_subtree_max={args.lane_subtree_max}"
@@ -384,11 +519,21 @@ def run_ours(args, workload):
                 "nominal_gbs": 64.0, "nominal": "PCIe Gen5 x16, one direction"}
         if world == 1 and not args.no_cpu_baseline:
             threads = os.cpu_count() or 1
-            m, dt, n_s, n_tot = cpu_sample_run(hg, texts, labeled, threads, target_s=15.0)
-            line["cpu_baseline"] = {"value": m / dt, "unit": "matches/s", "cores": threads, "kind": "port",
-                                    "sample": f"{n_s} of {n_tot} root edges, seeded random sample, "
-                                              f"{dt:.1f} s of oracle DFS"}
+            cm = cpu_measure(hg, texts, labeled, threads, sample, time_limit_s=15.0, per_root=sample is None)
+            line["cpu_baseline"] = {"value": cm["matches"] / cm["seconds"], "unit": "matches/s", "cores": threads,
+                                    "kind": "port", "sample": cm["sample"]}
+            if sample is None and args.root_limit == 0 and world == 1:
+                # per-root parity on the roots the CPU baseline sampled (plan 0)
+                idx = cm["roots"][0]
+                gpu = per_root_gpu[idx].astype(np.uint64)
+                bad = [int(i) for i, a, b in zip(idx, gpu, cm["per_root"][0]) if a != b]
+                ok = not bad
+                parity = {"roots_checked": int(len(idx)), "ok": ok, "mismatched_roots": bad[:16],
+                          "against": "oracle per-root counts on the CPU baseline's seeded root sample"}
+        line["parity"] = parity
         print(json.dumps(line), flush=True)
+        if not ok:
+            sys.exit(1)
     graph.close()
     ctx.close()
     if dist:

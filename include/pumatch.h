@@ -167,6 +167,16 @@ pm_status pm_gen_rmat(int64_t n, int64_t n_edges, double a, double b, double c,
                       uint64_t seed, uint64_t** rowptr, int32_t** colidx,
                       int64_t* n_adj, int32_t* max_degree);
 
+/* pm_gen_rmat computed on a device (the same arrays: the same draw sequence
+ * and the first n_edges distinct edges of it), for graphs whose host-side
+ * edge sort is too slow or too large -- the configured 65M-vertex, 1.8e9-edge
+ * graph.  Outputs are malloc'd host arrays (pm_host_free).  No counterpart in
+ * the reference, whose graphs are converted datasets
+ * (graph_converter/convert.sh). */
+pm_status pm_gen_rmat_device(int64_t n, int64_t n_edges, double a, double b, double c,
+                             uint64_t seed, int device, uint64_t** rowptr, int32_t** colidx,
+                             int64_t* n_adj, int32_t* max_degree);
+
 /* Uniform labels in [0, n_labels) (malloc'd uint32[n]). */
 pm_status pm_gen_labels(int64_t n, int n_labels, uint64_t seed, uint32_t** labels);
 
@@ -350,27 +360,30 @@ pm_status pm_mlp_set_weights(pm_mlp* m, const float* host_in);
 
 /* pm_match for callers that cannot allocate device memory (it has no
  * counterpart in the reference, whose driver allocates everything up front,
- * test.cu:59-154): code running in a
- * stream callback or another library's allocator-locked region, a service
- * whose device memory is budgeted and pooled elsewhere, or a framework that
- * owns the allocator.  It calls no cudaMalloc/cudaFree and no allocating
- * library routine: the caller passes the graph as DEVICE arrays (rowptr
- * uint64[n+1], colidx int32[n_adj], labels uint8[n] or NULL) and gets the
- * count in *count_out (host); the control block, root list and per-warp
- * arenas live in one static device array of PM_STATIC_SCRATCH_BYTES.
- *  - Limits: one plan; the root list plus one block of warp arenas
- *    (patterns' worst-case candidate sets, sized from max_degree) must fit
- *    the scratch, otherwise PM_ERR_INVALID says so; fewer warps run when
- *    the arenas only partly fit.  Per-root outputs, root orders, ranges and
- *    shards are not supported here.
+ * test.cu:59-154): a region that holds another library's allocator lock, a
+ * service whose device memory is budgeted and pooled elsewhere, or a
+ * framework that owns the allocator and forbids outside cudaMalloc calls.  It
+ * calls no cudaMalloc/cudaFree and no allocating library routine: the caller
+ * passes the graph as DEVICE arrays (rowptr uint64[n+1], colidx int32[n_adj],
+ * labels uint8[n] or NULL) and gets the count in *count_out (host); the
+ * control block, root list and per-warp arenas live in one static device
+ * array of PM_STATIC_SCRATCH_BYTES.  The launch's plan travels in its kernel
+ * parameters, so the scratch is all it shares with other launches.
+ *  - Limits: one plan; n below 2^31; the root list plus one block of warp
+ *    arenas (patterns' worst-case candidate sets, sized from max_degree)
+ *    must fit the scratch, otherwise PM_ERR_INVALID says so; fewer warps run
+ *    when the arenas only partly fit.  Per-root outputs, root orders, ranges
+ *    and shards are not supported here (PM_ERR_INVALID); every other
+ *    pm_run_opts field means what it means for pm_match.
  *  - The first call on a device looks up the scratch's device address
  *    (cudaGetSymbolAddress) with that device current; make that first call
  *    before any stream capture.
  *  - Every call shares the one scratch and clears what must start at zero;
  *    calls that overlap on the GPU (other threads, other streams) race on
  *    it -- serialize them.
- *  - stream: a cudaStream_t (NULL = legacy default stream); the call
- *    returns after the work on it is done.  stats_out->kernel_ms is 0. */
+ *  - stream: a cudaStream_t (NULL = legacy default stream).  The call
+ *    synchronizes that stream: it returns after the work on it is done, so
+ *    it is not for use inside a stream callback.  stats_out->kernel_ms is 0. */
 pm_status pm_match_static(const uint64_t* d_rowptr, const int32_t* d_colidx, const uint8_t* d_labels,
                           int64_t n, int64_t n_adj, int32_t max_degree, const pm_plan* plan,
                           const pm_run_opts* opts, void* stream, uint64_t* count_out,

@@ -31,6 +31,8 @@
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+#include <time.h>
+#include <math.h>
 
 /* ------------------------------------------------------------------ */
 /* Plan compiler: restates PatternPreprocessor (src/pattern.h:48-355). */
@@ -504,16 +506,158 @@ uint64_t orc_count_mt(const orc_graph* g, const orc_plan* p, const int32_t* root
   return total;
 }
 
-/* ------------------------------------------------------------------ */
-/* Knuth estimator (workload sizing only).                              */
-/* ------------------------------------------------------------------ */
-
 static uint64_t sm64(uint64_t* s) {
   uint64_t z = (*s += 0x9E3779B97F4A7C15ull);
   z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
   z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
   return z ^ (z >> 31);
 }
+
+/* ------------------------------------------------------------------ */
+/* Split runs: one root's DFS divided over threads at level 1's main    */
+/* slot.  Same DFS (extend) per piece, so per-root counts are those of  */
+/* orc_count; only the work division differs.                           */
+/* ------------------------------------------------------------------ */
+
+typedef struct {
+  const orc_graph* g;
+  const orc_plan* p;
+  const int32_t* roots;
+  const int64_t* item_root; /* per item: root index; item_k: level-1 candidate (-1 = whole root) */
+  const int32_t* item_k;
+  int64_t nitems;
+  int T;
+  int64_t maxdeg;
+  double deadline; /* CLOCK_MONOTONIC seconds, 0 = none */
+  volatile int64_t* cursor;
+  volatile int64_t* done;
+  uint64_t* per_root;
+  uint64_t total;
+  orc_stats st;
+} split_arg;
+
+static double mono_s(void) {
+  struct timespec ts;
+  clock_gettime(CLOCK_MONOTONIC, &ts);
+  return (double)ts.tv_sec + 1e-9 * (double)ts.tv_nsec;
+}
+
+static void* split_worker(void* v) {
+  split_arg* a = (split_arg*)v;
+  dfs_t d;
+  dfs_init(&d, a->g, a->p, a->T, a->maxdeg);
+  for (;;) {
+    if (a->deadline > 0 && mono_s() >= a->deadline) break;
+    const int64_t i = __atomic_fetch_add(a->cursor, 1, __ATOMIC_RELAXED);
+    if (i >= a->nitems) break;
+    const int64_t r = a->item_root[i];
+    const int k = a->item_k[i];
+    d.path[0] = a->roots[2 * r];
+    d.path[1] = a->roots[2 * r + 1];
+    uint64_t c;
+    if (k < 0) {
+      c = extend(&d, 1);
+    } else {
+      /* level 1 again for this root (its set operations were counted once
+       * by the caller), then the subtree of candidate k */
+      const orc_stats keep = d.st;
+      const int b = a->p->level_begin[1], e = a->p->level_begin[2];
+      for (int s = b; s < e; s++) compute_slot(&d, 1, s);
+      d.st = keep;
+      d.path[2] = d.buf[b][k];
+      c = extend(&d, 2);
+    }
+    if (a->per_root) __atomic_fetch_add(&a->per_root[r], c, __ATOMIC_RELAXED);
+    a->total += c;
+    __atomic_fetch_add(a->done, 1, __ATOMIC_RELAXED);
+  }
+  a->st = d.st;
+  dfs_free(&d);
+  return NULL;
+}
+
+uint64_t orc_count_split(const orc_graph* g, const orc_plan* p, const int32_t* roots, int64_t nroots,
+                         int truncate, int nthreads, double time_limit_s, uint64_t shuffle_seed,
+                         uint64_t* per_root, int64_t* items_done, int64_t* items_total, orc_stats* st) {
+  if (nthreads < 1) nthreads = 1;
+  const int64_t md = max_degree(g);
+  const double t0 = mono_s();
+  orc_stats agg = {0, 0, 0};
+  /* items: (root, level-1 candidate) for plans of 4+ vertices, whole roots otherwise */
+  int64_t nitems = 0, cap = nroots > 0 ? nroots : 1;
+  int64_t* item_root = (int64_t*)malloc(sizeof(int64_t) * (size_t)cap);
+  int32_t* item_k = (int32_t*)malloc(sizeof(int32_t) * (size_t)cap);
+  uint64_t* pr = per_root ? per_root : (uint64_t*)calloc((size_t)cap, sizeof(uint64_t));
+  if (per_root) memset(per_root, 0, sizeof(uint64_t) * (size_t)nroots);
+  {
+    dfs_t d;
+    dfs_init(&d, g, p, truncate, md);
+    const int deep = p->nnodes > 3;
+    for (int64_t r = 0; r < nroots; r++) {
+      int64_t m = 1;
+      if (deep) {
+        d.path[0] = roots[2 * r];
+        d.path[1] = roots[2 * r + 1];
+        const int b = p->level_begin[1], e = p->level_begin[2];
+        for (int s = b; s < e; s++) compute_slot(&d, 1, s);
+        m = d.size[b];
+      }
+      d.st.alg_bytes += 8;
+      d.st.roots++;
+      if (nitems + m > cap) {
+        while (nitems + m > cap) cap *= 2;
+        item_root = (int64_t*)realloc(item_root, sizeof(int64_t) * (size_t)cap);
+        item_k = (int32_t*)realloc(item_k, sizeof(int32_t) * (size_t)cap);
+      }
+      for (int64_t k = 0; k < m; k++) {
+        item_root[nitems] = r;
+        item_k[nitems] = deep ? (int32_t)k : -1;
+        nitems++;
+      }
+    }
+    agg = d.st;
+    dfs_free(&d);
+  }
+  if (shuffle_seed) {
+    uint64_t s = shuffle_seed;
+    for (int64_t i = nitems - 1; i > 0; i--) {
+      const int64_t j = (int64_t)(sm64(&s) % (uint64_t)(i + 1));
+      const int64_t tr = item_root[i]; item_root[i] = item_root[j]; item_root[j] = tr;
+      const int32_t tk = item_k[i]; item_k[i] = item_k[j]; item_k[j] = tk;
+    }
+  }
+  int64_t cursor = 0, done = 0;
+  split_arg* args = (split_arg*)calloc((size_t)nthreads, sizeof(split_arg));
+  pthread_t* th = (pthread_t*)calloc((size_t)nthreads, sizeof(pthread_t));
+  for (int t = 0; t < nthreads; t++) {
+    split_arg* a = &args[t];
+    a->g = g; a->p = p; a->roots = roots; a->item_root = item_root; a->item_k = item_k;
+    a->nitems = nitems; a->T = truncate; a->maxdeg = md;
+    a->deadline = time_limit_s > 0 ? t0 + time_limit_s : 0;
+    a->cursor = &cursor; a->done = &done; a->per_root = pr;
+    pthread_create(&th[t], NULL, split_worker, a);
+  }
+  uint64_t total = 0;
+  for (int t = 0; t < nthreads; t++) {
+    pthread_join(th[t], NULL);
+    total += args[t].total;
+    agg.set_ops += args[t].st.set_ops;
+    agg.alg_bytes += args[t].st.alg_bytes;
+  }
+  if (items_done) *items_done = done;
+  if (items_total) *items_total = nitems;
+  if (st) *st = agg;
+  if (!per_root) free(pr);
+  free(args);
+  free(th);
+  free(item_root);
+  free(item_k);
+  return total;
+}
+
+/* ------------------------------------------------------------------ */
+/* Knuth estimator (workload sizing only).                              */
+/* ------------------------------------------------------------------ */
 
 void orc_estimate(const orc_graph* g, const orc_plan* p, const int32_t* roots, int64_t nroots,
                   int probes, uint64_t seed, double* est_setops, double* est_bytes,
@@ -552,3 +696,204 @@ void orc_estimate(const orc_graph* g, const orc_plan* p, const int32_t* roots, i
   *est_bytes = by * f;
   *est_count = ct * f;
 }
+
+/* ------------------------------------------------------------------ */
+/* Seeded graph generators.  Restate the workload definitions the       */
+/* product's generators implement (splitmix64-seeded xoshiro256**       */
+/* streams, one stream per batch of 65,536 draws, the first m distinct  */
+/* undirected edges of the draw sequence, sorted CSR), sequentially and */
+/* with a hash set instead of sorted rounds: the same edge set.  Used   */
+/* by the CPU measurement arm so that it builds its inputs without the  */
+/* product library.                                                     */
+/* ------------------------------------------------------------------ */
+
+typedef struct { uint64_t s[4]; } orc_rng;
+
+static void rng_init(orc_rng* r, uint64_t seed, uint64_t stream) {
+  uint64_t x = seed ^ (stream * 0xD1B54A32D192ED03ull);
+  for (int i = 0; i < 4; i++) r->s[i] = sm64(&x);
+}
+static inline uint64_t rotl64(uint64_t x, int k) { return (x << k) | (x >> (64 - k)); }
+static inline uint64_t rng_next(orc_rng* r) {
+  uint64_t* s = r->s;
+  const uint64_t res = rotl64(s[1] * 5, 7) * 9;
+  const uint64_t t = s[1] << 17;
+  s[2] ^= s[0]; s[3] ^= s[1]; s[1] ^= s[2]; s[0] ^= s[3];
+  s[2] ^= t; s[3] = rotl64(s[3], 45);
+  return res;
+}
+static inline double rng_uniform(orc_rng* r) { return (double)(rng_next(r) >> 11) * (1.0 / 9007199254740992.0); }
+static inline uint32_t rng_below(orc_rng* r, uint32_t n) {
+  return (uint32_t)(((rng_next(r) >> 32) * (uint64_t)n) >> 32);
+}
+
+/* open-addressing set of edge keys (key + 1 stored, 0 = empty) */
+typedef struct { uint64_t* t; uint64_t mask; int64_t size; } keyset;
+
+static int keyset_add(keyset* k, uint64_t key) {
+  uint64_t h = (key * 0x9E3779B97F4A7C15ull) >> 20;
+  for (;;) {
+    h &= k->mask;
+    if (k->t[h] == 0) { k->t[h] = key + 1; k->size++; return 1; }
+    if (k->t[h] == key + 1) return 0;
+    h++;
+  }
+}
+
+static int cmp_u64(const void* a, const void* b) {
+  const uint64_t x = *(const uint64_t*)a, y = *(const uint64_t*)b;
+  return x < y ? -1 : x > y;
+}
+static int cmp_i32(const void* a, const void* b) {
+  const int32_t x = *(const int32_t*)a, y = *(const int32_t*)b;
+  return x < y ? -1 : x > y;
+}
+
+/* draw(ctx, rng) returns an edge key (lo << 32 | hi, lo < hi) or UINT64_MAX */
+typedef uint64_t (*draw_fn)(void* ctx, orc_rng* r);
+
+static int gen_edges(int64_t n, int64_t m, uint64_t seed, draw_fn draw, void* ctx, uint64_t** rowptr_out,
+                     int32_t** colidx_out, int64_t* nadj_out) {
+  uint64_t cap = 1;
+  while (cap < (uint64_t)(2 * m + 16)) cap <<= 1;
+  keyset ks = {(uint64_t*)calloc(cap, sizeof(uint64_t)), cap - 1, 0};
+  uint64_t* keys = (uint64_t*)malloc(sizeof(uint64_t) * (size_t)(m > 0 ? m : 1));
+  if (!ks.t || !keys) return -1;
+  const int64_t kBatch = 1 << 16;
+  for (uint64_t batch = 1; ks.size < m; batch++) {
+    if (batch > (uint64_t)(64 * (m / kBatch + 2) + 4096)) break; /* too dense */
+    orc_rng r;
+    rng_init(&r, seed, batch);
+    for (int64_t k = 0; k < kBatch && ks.size < m; k++) {
+      const uint64_t key = draw(ctx, &r);
+      if (key != UINT64_MAX && keyset_add(&ks, key)) keys[ks.size - 1] = key;
+    }
+  }
+  free(ks.t);
+  if (ks.size != m) { free(keys); return -2; }
+  qsort(keys, (size_t)m, sizeof(uint64_t), cmp_u64);
+  uint64_t* rowptr = (uint64_t*)calloc((size_t)n + 1, sizeof(uint64_t));
+  for (int64_t e = 0; e < m; e++) { rowptr[(keys[e] >> 32) + 1]++; rowptr[(keys[e] & 0xffffffffu) + 1]++; }
+  for (int64_t v = 0; v < n; v++) rowptr[v + 1] += rowptr[v];
+  const int64_t nadj = (int64_t)rowptr[n];
+  int32_t* colidx = (int32_t*)malloc(sizeof(int32_t) * (size_t)(nadj > 0 ? nadj : 1));
+  uint64_t* fill = (uint64_t*)malloc(sizeof(uint64_t) * (size_t)(n > 0 ? n : 1));
+  memcpy(fill, rowptr, sizeof(uint64_t) * (size_t)n);
+  for (int64_t e = 0; e < m; e++) {
+    const uint32_t lo = (uint32_t)(keys[e] >> 32), hi = (uint32_t)(keys[e] & 0xffffffffu);
+    colidx[fill[lo]++] = (int32_t)hi;
+    colidx[fill[hi]++] = (int32_t)lo;
+  }
+  for (int64_t v = 0; v < n; v++)
+    qsort(colidx + rowptr[v], (size_t)(rowptr[v + 1] - rowptr[v]), sizeof(int32_t), cmp_i32);
+  free(fill);
+  free(keys);
+  *rowptr_out = rowptr;
+  *colidx_out = colidx;
+  *nadj_out = nadj;
+  return 0;
+}
+
+static inline uint64_t edge_key32(uint32_t u, uint32_t v) {
+  return u < v ? ((uint64_t)u << 32 | v) : ((uint64_t)v << 32 | u);
+}
+
+typedef struct { uint32_t n; const double* prob; const uint32_t* alias; } cl_ctx;
+
+static uint64_t cl_draw(void* c, orc_rng* r) {
+  const cl_ctx* x = (const cl_ctx*)c;
+  uint32_t e[2];
+  for (int q = 0; q < 2; q++) {
+    const uint32_t i = rng_below(r, x->n);
+    e[q] = rng_uniform(r) < x->prob[i] ? i : x->alias[i];
+  }
+  return e[0] == e[1] ? UINT64_MAX : edge_key32(e[0], e[1]);
+}
+
+/* Chung-Lu: expected degrees w_i ~ (i + i0)^(-1/(gamma-1)) scaled to sum 2m
+ * and capped at max_w; both endpoints drawn proportional to w (Vose alias
+ * table, built in the same order of operations so the doubles agree). */
+int orc_gen_chung_lu(int64_t n, int64_t m, double gamma, double i0, double max_w, uint64_t seed,
+                     uint64_t** rowptr, int32_t** colidx, int64_t* nadj) {
+  if (n < 2 || n > INT_MAX || m < 0 || gamma <= 1.0) return -1;
+  double* w = (double*)malloc(sizeof(double) * (size_t)n);
+  double sum = 0;
+  for (int64_t i = 0; i < n; i++) { w[i] = pow((double)i + i0, -1.0 / (gamma - 1.0)); sum += w[i]; }
+  for (int64_t i = 0; i < n; i++) { w[i] *= 2.0 * (double)m / sum; if (max_w > 0 && w[i] > max_w) w[i] = max_w; }
+  double tot = 0;
+  for (int64_t i = 0; i < n; i++) tot += w[i];
+  double* prob = (double*)malloc(sizeof(double) * (size_t)n);
+  uint32_t* alias = (uint32_t*)calloc((size_t)n, sizeof(uint32_t));
+  int64_t* small = (int64_t*)malloc(sizeof(int64_t) * (size_t)n);
+  int64_t* large = (int64_t*)malloc(sizeof(int64_t) * (size_t)n);
+  int64_t ns = 0, nl = 0;
+  for (int64_t i = 0; i < n; i++) {
+    prob[i] = w[i] * (double)n / tot;
+    if (prob[i] < 1.0) small[ns++] = i; else large[nl++] = i;
+  }
+  while (ns > 0 && nl > 0) {
+    const int64_t s = small[--ns];
+    const int64_t l = large[nl - 1];
+    alias[s] = (uint32_t)l;
+    prob[l] = prob[l] + prob[s] - 1.0;
+    if (prob[l] < 1.0) { nl--; small[ns++] = l; }
+  }
+  for (int64_t i = 0; i < nl; i++) prob[large[i]] = 1.0;
+  for (int64_t i = 0; i < ns; i++) prob[small[i]] = 1.0;
+  free(small);
+  free(large);
+  free(w);
+  cl_ctx c = {(uint32_t)n, prob, alias};
+  const int rc = gen_edges(n, m, seed, cl_draw, &c, rowptr, colidx, nadj);
+  free(prob);
+  free(alias);
+  return rc;
+}
+
+typedef struct { int scale; uint64_t n; uint32_t ta, tb, tc; } rmat_ctx;
+
+static uint64_t rmat_draw(void* c, orc_rng* r) {
+  const rmat_ctx* x = (const rmat_ctx*)c;
+  uint64_t u = 0, v = 0, bits = 0;
+  for (int l = 0; l < x->scale; l++) {
+    if ((l & 3) == 0) bits = rng_next(r);
+    const uint32_t q = (uint32_t)(bits & 0xffff);
+    bits >>= 16;
+    const uint32_t bu = q >= x->tb, bv = (q >= x->ta && q < x->tb) || q >= x->tc;
+    u = (u << 1) | bu;
+    v = (v << 1) | bv;
+  }
+  return (u >= x->n || v >= x->n || u == v) ? UINT64_MAX : edge_key32((uint32_t)u, (uint32_t)v);
+}
+
+/* R-MAT: per level one 16-bit draw picks the quadrant (a, b, c, d); ids >= n
+ * and self-loops are rejected. */
+int orc_gen_rmat(int64_t n, int64_t m, double a, double b, double c, uint64_t seed, uint64_t** rowptr,
+                 int32_t** colidx, int64_t* nadj) {
+  if (n < 2 || n > INT_MAX || m < 0 || a < 0 || b < 0 || c < 0 || a + b + c > 1.0) return -1;
+  rmat_ctx x;
+  x.scale = 0;
+  while ((1ll << x.scale) < n) x.scale++;
+  x.n = (uint64_t)n;
+  x.ta = (uint32_t)llround(a * 65536.0);
+  x.tb = (uint32_t)llround((a + b) * 65536.0);
+  x.tc = (uint32_t)llround((a + b + c) * 65536.0);
+  return gen_edges(n, m, seed, rmat_draw, &x, rowptr, colidx, nadj);
+}
+
+/* Uniform labels in [0, n_labels): vertex block b of 65,536 from stream b+1. */
+int orc_gen_labels(int64_t n, int n_labels, uint64_t seed, uint32_t** labels) {
+  if (n < 0 || n_labels < 1 || n_labels > 32) return -1;
+  uint32_t* lab = (uint32_t*)malloc(sizeof(uint32_t) * (size_t)(n > 0 ? n : 1));
+  const int64_t kBlock = 1 << 16;
+  for (int64_t b = 0; b < (n + kBlock - 1) / kBlock; b++) {
+    orc_rng r;
+    rng_init(&r, seed, (uint64_t)b + 1);
+    const int64_t e = (b + 1) * kBlock < n ? (b + 1) * kBlock : n;
+    for (int64_t v = b * kBlock; v < e; v++) lab[v] = rng_below(&r, (uint32_t)n_labels);
+  }
+  *labels = lab;
+  return 0;
+}
+
+void orc_free(void* p) { free(p); }

@@ -69,6 +69,25 @@ uint64_t orc_count_mt(const orc_graph* g, const orc_plan* p, const int32_t* root
                       int64_t begin, int64_t end, int truncate, int nthreads,
                       orc_stats* st);
 
+/* Per-root counts of roots[0, nroots) with each root's DFS divided over
+ * nthreads at the candidates of level 1's main slot (the same DFS per piece,
+ * so the counts are orc_count's).  Pieces run in a shuffled order when
+ * shuffle_seed != 0; with time_limit_s > 0 the run stops at the limit and the
+ * counts cover the pieces done (*items_done of *items_total). */
+uint64_t orc_count_split(const orc_graph* g, const orc_plan* p, const int32_t* roots, int64_t nroots,
+                         int truncate, int nthreads, double time_limit_s, uint64_t shuffle_seed,
+                         uint64_t* per_root, int64_t* items_done, int64_t* items_total, orc_stats* st);
+
+/* Seeded generators with the workload definitions of the product's
+ * generators (same edge sets), for inputs built without the product library.
+ * Outputs are malloc'd; release with orc_free.  0 on success. */
+int orc_gen_chung_lu(int64_t n, int64_t m, double gamma, double i0, double max_w, uint64_t seed,
+                     uint64_t** rowptr, int32_t** colidx, int64_t* nadj);
+int orc_gen_rmat(int64_t n, int64_t m, double a, double b, double c, uint64_t seed, uint64_t** rowptr,
+                 int32_t** colidx, int64_t* nadj);
+int orc_gen_labels(int64_t n, int n_labels, uint64_t seed, uint32_t** labels);
+void orc_free(void* p);
+
 /* Knuth's random-probe estimator of the DFS tree: estimates the number of set
  * operations and algorithmic bytes of a full run (workload sizing only). */
 void orc_estimate(const orc_graph* g, const orc_plan* p, const int32_t* roots, int64_t nroots,

@@ -71,6 +71,19 @@ def lib() -> C.CDLL:
                                    C.c_uint64, C.POINTER(C.c_double), C.POINTER(C.c_double),
                                    C.POINTER(C.c_double)]
         L.orc_estimate.restype = None
+        L.orc_count_split.argtypes = [C.POINTER(OrcGraph), C.POINTER(OrcPlan), C.c_void_p, C.c_int64, C.c_int,
+                                      C.c_int, C.c_double, C.c_uint64, C.c_void_p, C.POINTER(C.c_int64),
+                                      C.POINTER(C.c_int64), C.POINTER(OrcStats)]
+        L.orc_count_split.restype = C.c_uint64
+        for name in ("orc_gen_chung_lu", "orc_gen_rmat"):
+            f = getattr(L, name)
+            f.argtypes = [C.c_int64, C.c_int64, C.c_double, C.c_double, C.c_double, C.c_uint64,
+                          C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.POINTER(C.c_int64)]
+            f.restype = C.c_int
+        L.orc_gen_labels.argtypes = [C.c_int64, C.c_int, C.c_uint64, C.POINTER(C.c_void_p)]
+        L.orc_gen_labels.restype = C.c_int
+        L.orc_free.argtypes = [C.c_void_p]
+        L.orc_free.restype = None
         _lib = L
     return _lib
 
@@ -125,6 +138,57 @@ def total(g: Graph, text: str, labeled: bool, truncate: int = 0, threads: int = 
     r = roots(g, p)
     c, _ = count(g, p, r, truncate=truncate, threads=threads)
     return c if labeled else c * p.multiplicity
+
+
+def count_split(g: Graph, p: OrcPlan, rts: np.ndarray, threads: int = 1, time_limit_s: float = 0.0,
+                shuffle_seed: int = 0, truncate: int = 0):
+    """Raw per-root counts of the roots in `rts`, each root's DFS divided over
+    `threads` at the candidates of level 1 (pieces in a seeded shuffled order
+    when shuffle_seed != 0).  With time_limit_s > 0 the run stops at the limit:
+    the counts then cover the pieces done.  Returns (total, per_root,
+    pieces_done, pieces_total, stats)."""
+    rts = np.ascontiguousarray(rts, dtype=np.int32)
+    pr = np.zeros(max(len(rts), 1), dtype=np.uint64)
+    done, tot = C.c_int64(), C.c_int64()
+    st = OrcStats()
+    c = lib().orc_count_split(C.byref(g.g), C.byref(p), rts.ctypes.data, len(rts), truncate, threads,
+                              float(time_limit_s), shuffle_seed, pr.ctypes.data, C.byref(done), C.byref(tot),
+                              C.byref(st))
+    return int(c), pr[:len(rts)], done.value, tot.value, {"set_ops": st.set_ops, "alg_bytes": st.alg_bytes,
+                                                          "roots": st.roots}
+
+
+def _take(ptr: C.c_void_p, n: int, dtype) -> np.ndarray:
+    if n == 0:
+        lib().orc_free(ptr)
+        return np.zeros(0, dtype=dtype)
+    buf = (C.c_char * (n * np.dtype(dtype).itemsize)).from_address(ptr.value)
+    out = np.frombuffer(buf, dtype=dtype).copy()
+    lib().orc_free(ptr)
+    return out
+
+
+def gen_chung_lu(n: int, m: int, gamma: float, i0: float, max_w: float, seed: int):
+    """(rowptr, colidx) of the seeded Chung-Lu graph (the product generator's definition)."""
+    rp, ci, nadj = C.c_void_p(), C.c_void_p(), C.c_int64()
+    if lib().orc_gen_chung_lu(n, m, gamma, i0, max_w, seed, C.byref(rp), C.byref(ci), C.byref(nadj)) != 0:
+        raise ValueError("orc_gen_chung_lu failed")
+    return _take(rp, n + 1, np.uint64), _take(ci, nadj.value, np.int32)
+
+
+def gen_rmat(n: int, m: int, a: float, b: float, c: float, seed: int):
+    """(rowptr, colidx) of the seeded R-MAT graph (the product generator's definition)."""
+    rp, ci, nadj = C.c_void_p(), C.c_void_p(), C.c_int64()
+    if lib().orc_gen_rmat(n, m, a, b, c, seed, C.byref(rp), C.byref(ci), C.byref(nadj)) != 0:
+        raise ValueError("orc_gen_rmat failed")
+    return _take(rp, n + 1, np.uint64), _take(ci, nadj.value, np.int32)
+
+
+def gen_labels(n: int, n_labels: int, seed: int) -> np.ndarray:
+    lb = C.c_void_p()
+    if lib().orc_gen_labels(n, n_labels, seed, C.byref(lb)) != 0:
+        raise ValueError("orc_gen_labels failed")
+    return _take(lb, n, np.uint32)
 
 
 def estimate(g: Graph, p: OrcPlan, rts: np.ndarray, probes: int = 2000, seed: int = 7):

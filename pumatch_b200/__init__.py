@@ -107,6 +107,8 @@ SIGNATURES = {
                                   _PP, _PP, C.POINTER(C.c_int64), C.POINTER(C.c_int32)]),
     "pm_gen_rmat": (C.c_int, [C.c_int64, C.c_int64, C.c_double, C.c_double, C.c_double, C.c_uint64,
                               _PP, _PP, C.POINTER(C.c_int64), C.POINTER(C.c_int32)]),
+    "pm_gen_rmat_device": (C.c_int, [C.c_int64, C.c_int64, C.c_double, C.c_double, C.c_double, C.c_uint64,
+                                     C.c_int, _PP, _PP, C.POINTER(C.c_int64), C.POINTER(C.c_int32)]),
     "pm_gen_labels": (C.c_int, [C.c_int64, C.c_int, C.c_uint64, _PP]),
     "pm_plan_compile": (C.c_int, [C.c_char_p, C.c_int, _PP]),
     "pm_plan_compile_text": (C.c_int, [C.c_char_p, C.c_int, _PP]),
@@ -261,11 +263,17 @@ def gen_chung_lu(n: int, n_edges: int, gamma: float = 2.1, i0: float = 10.0, max
 
 
 def gen_rmat(n: int, n_edges: int, a: float = 0.57, b: float = 0.19, c: float = 0.19,
-             seed: int = 2) -> HostGraph:
-    """Seeded R-MAT graph (ids >= n rejected; sorted, deduplicated, no self-loops)."""
+             seed: int = 2, device: Optional[int] = None) -> HostGraph:
+    """Seeded R-MAT graph (ids >= n rejected; sorted, deduplicated, no self-loops).
+    device: compute it on that GPU (same arrays), for graphs too large to sort
+    on the host quickly."""
     rp, ci, nadj, md = C.c_void_p(), C.c_void_p(), C.c_int64(), C.c_int32()
-    _check(lib().pm_gen_rmat(n, n_edges, a, b, c, seed, C.byref(rp), C.byref(ci), C.byref(nadj),
-                             C.byref(md)))
+    if device is not None:
+        _check(lib().pm_gen_rmat_device(n, n_edges, a, b, c, seed, device, C.byref(rp), C.byref(ci),
+                                        C.byref(nadj), C.byref(md)))
+    else:
+        _check(lib().pm_gen_rmat(n, n_edges, a, b, c, seed, C.byref(rp), C.byref(ci), C.byref(nadj),
+                                 C.byref(md)))
     return HostGraph(_take(rp, n + 1, np.uint64), _take(ci, nadj.value, np.int32))
 
 

@@ -24,7 +24,7 @@ CUDA = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA, "bin", "nvcc")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-CU_SOURCES = ["pm_device.cu", "pm_paging.cu", "pm_learn.cu"]
+CU_SOURCES = ["pm_device.cu", "pm_paging.cu", "pm_learn.cu", "pm_gen.cu"]
 CPP_SOURCES = ["pm_host.cpp"]
 HEADERS = ["pm_common.h", "pm_device.cuh"]
 

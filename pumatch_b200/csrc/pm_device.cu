@@ -59,8 +59,6 @@ static constexpr unsigned FULL = 0xffffffffu;
 // Device helpers
 // =====================================================================
 
-__constant__ DPlan c_plans[PM_MAX_BATCH];
-
 __device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
 __device__ __forceinline__ unsigned long long global_ns() {
   unsigned long long t;
@@ -115,6 +113,11 @@ struct MatchArgs {
   unsigned long long timeout_ns;  // hard limit on the launch; idle warps also give
                                   // up after this long without a heartbeat
   DPaging pg;
+  // the launch's plans, in the kernel's own parameter block: every launch
+  // carries its own copy, so launches that overlap on a device (other
+  // contexts, prepared queries, the allocation-free entry) never see each
+  // other's plans
+  DPlan plans[PM_MAX_BATCH];
 };
 
 enum { ST_SETOPS = 0, ST_BYTES = 1, ST_ROOTS = 2, ST_SPLITS = 3, ST_HITS = 4, ST_MISSES = 5,
@@ -1095,7 +1098,7 @@ __device__ bool take_donation(const MatchArgs& a, Donation& d) {
 // some spills); MINB = 3: 85 registers, three blocks; MINB = 1: up to 128
 // registers, no spills, fewer warps.
 template <bool LABELED, bool PAGED, int MINB>
-__global__ void __launch_bounds__(MINB == 1 ? 512 : 256, MINB) match_kernel(MatchArgs a) {
+__global__ void __launch_bounds__(MINB == 1 ? 512 : 256, MINB) match_kernel(const __grid_constant__ MatchArgs a) {
   extern __shared__ WarpState smem_state[];
   const int lane = lane_id();
   const int wib = threadIdx.x >> 5;
@@ -1112,7 +1115,7 @@ __global__ void __launch_bounds__(MINB == 1 ? 512 : 256, MINB) match_kernel(Matc
   int exhausted = 0;
   // phase 1: root chunks from the per-plan cursors
   while (exhausted < np && !w.err) {
-    const DPlan& P = c_plans[p];
+    const DPlan& P = a.plans[p];
     const unsigned long long nchunks = (unsigned long long)((P.nroots + a.chunk - 1) / a.chunk);
     unsigned long long c = 0;
     if (lane == 0) c = atomicAdd(&a.cursors[p], 1ull);
@@ -1156,7 +1159,7 @@ __global__ void __launch_bounds__(MINB == 1 ? 512 : 256, MINB) match_kernel(Matc
     Donation item;
     if (take_donation(a, item)) {
       const unsigned long long t_item = global_ns();
-      const DPlan& P = c_plans[item.plan];
+      const DPlan& P = a.plans[item.plan];
       const int2 e = P.roots[item.root];
       if (lane == 0) {
         S.path[0] = e.x;
@@ -1438,6 +1441,12 @@ RootFilter to_filter(const Plan& p) {
   return f;
 }
 
+// Parent-set limit of the two-level lane scheme from the run options: 0 =
+// default (64), negative = never, else capped at the shared staging size.
+int lane_subtree_limit(const pm_run_opts& o) {
+  return o.lane_subtree_max < 0 ? 0 : (o.lane_subtree_max == 0 ? 64 : std::min(o.lane_subtree_max, PM_SB_MAX));
+}
+
 // Worst-case arena words one warp needs for a plan: every materialised slot
 // is at most its first operand, itself at most a max-degree list.
 int64_t arena_words_for(const Plan& p, int32_t maxdeg, int T) {
@@ -1453,7 +1462,7 @@ namespace pm {
 // mapped host memory).
 pm_status compute_maxnbrdeg(pm_graph* g, const int32_t* colidx) {
   if (g->n > 0) {
-    (void)cudaGetLastError();  // drop a stale error from an earlier call
+    PM_CK_PENDING("max neighbour degree");
     maxnbrdeg_kernel<<<2048, 256>>>(g->d_rowptr, colidx, g->n, g->d_maxnbrdeg);
     CK(cudaGetLastError());
     CK(cudaDeviceSynchronize());
@@ -1467,7 +1476,7 @@ static pm_status graph_finish(pm_graph* g) {
   CK(cudaMalloc(&g->d_maxnbrdeg, sizeof(int32_t) * std::max<int64_t>(g->n, 1)));
   g->device_bytes += sizeof(int32_t) * g->n;
   if (g->n > 0 && g->residency == PM_RESIDENT_HBM) {
-    (void)cudaGetLastError();  // drop a stale error from an earlier call
+    PM_CK_PENDING("max neighbour degree");
     maxnbrdeg_kernel<<<2048, 256>>>(g->d_rowptr, g->d_colidx, g->n, g->d_maxnbrdeg);
     CK(cudaGetLastError());
     CK(cudaDeviceSynchronize());
@@ -1477,7 +1486,7 @@ static pm_status graph_finish(pm_graph* g) {
     CK(cudaMalloc(&g->d_colidx_lab, sizeof(int32_t) * std::max<int64_t>(g->nadj, 1)));
     CK(cudaMalloc(&g->d_lab_off, sizeof(int32_t) * (size_t)g->n * g->nl1));
     g->device_bytes += sizeof(int32_t) * ((size_t)g->nadj + (size_t)g->n * g->nl1);
-    (void)cudaGetLastError();  // drop a stale error from an earlier call
+    PM_CK_PENDING("label grouping");
     label_group_kernel<<<2048, 256>>>(g->d_rowptr, g->d_colidx, g->d_labels, 0, g->n, g->nl1, g->d_colidx_lab, 0,
                                       g->d_lab_off);
     CK(cudaGetLastError());
@@ -1499,13 +1508,13 @@ static pm_status paged_group_labels(pm_graph* g, const uint64_t* h_rowptr) {
   g->device_bytes += sizeof(int32_t) * (size_t)g->n * g->nl1;
   const int64_t chunk = std::max<int64_t>(g->maxdeg, std::min<int64_t>(std::max<int64_t>(g->nadj, 1), 64ll << 20));
   int32_t* tmp = nullptr;
+  PM_CK_PENDING("label grouping");
   CK(cudaMalloc(&tmp, sizeof(int32_t) * (size_t)std::max<int64_t>(chunk, 1)));
   pm_status st = PM_OK;
   for (int64_t v0 = 0; v0 < g->n && st == PM_OK;) {
     int64_t v1 = v0;
     while (v1 < g->n && (int64_t)(h_rowptr[v1 + 1] - h_rowptr[v0]) <= chunk) v1++;
     const uint64_t b0 = h_rowptr[v0], len = h_rowptr[v1] - b0;
-    (void)cudaGetLastError();  // drop a stale error from an earlier call
     label_group_kernel<<<2048, 256>>>(g->d_rowptr, g->h_colidx_dev, g->d_labels, v0, v1, g->nl1, tmp, b0,
                                       g->d_lab_off);
     cudaError_t e = cudaGetLastError();
@@ -1729,7 +1738,7 @@ static pm_status build_roots(pm_ctx* c, const pm_graph* g, const Plan& p, size_t
   }
   const RootFilter f = to_filter(p);
   const int32_t* colidx = g->residency == PM_RESIDENT_HBM ? g->d_colidx : g->h_colidx_dev;
-  (void)cudaGetLastError();  // drop a stale error from an earlier call
+  PM_CK_PENDING("root filter");
   roots_kernel<false><<<4 * c->nsm, 256, 0, c->stream>>>(g->d_rowptr, colidx, g->d_labels, g->d_maxnbrdeg, n, f,
                                                           c->d_vcount, nullptr, nullptr);
   CK(cudaGetLastError());
@@ -1756,7 +1765,7 @@ static pm_status build_roots(pm_ctx* c, const pm_graph* g, const Plan& p, size_t
     *roots_buf = nr;
     *roots_bytes = want + want / 4;
   }
-  (void)cudaGetLastError();  // drop a stale error from an earlier call
+  PM_CK_PENDING("root filter");
   roots_kernel<true><<<4 * c->nsm, 256, 0, c->stream>>>(g->d_rowptr, colidx, g->d_labels, g->d_maxnbrdeg, n, f,
                                                          nullptr, c->d_voff, *roots_buf + offset_roots);
   CK(cudaGetLastError());
@@ -1812,7 +1821,7 @@ struct Launch {
   MatchArgs a;
   int blocks = 0, threads = 0;
   size_t smem = 0;
-  void (*kfn)(MatchArgs) = nullptr;
+  void (*kfn)(const MatchArgs) = nullptr;
   int64_t warps = 0;
   size_t ctl_words = 0;
   unsigned int active0 = 0;  // initial active-warp count (host staging)
@@ -1928,7 +1937,7 @@ static pm_status setup_launch(pm_ctx* c, const pm_graph* g, const pm_plan* const
   a.lab_off = g->d_lab_off;
   a.host_sorted = (g->residency == PM_RESIDENT_PAGED && g->d_lab_off) ? g->h_colidx_dev : nullptr;
   a.leaf_flat = o.leaf_per_lane ? 0 : 1;
-  a.lane_subtree_max = o.lane_subtree_max < 0 ? 0 : (o.lane_subtree_max == 0 ? 64 : std::min(o.lane_subtree_max, PM_SB_MAX));
+  a.lane_subtree_max = lane_subtree_limit(o);
   a.nl1 = g->nl1;
   a.n = (int32_t)g->n;
   a.nplans = nplans;
@@ -1959,6 +1968,7 @@ static pm_status setup_launch(pm_ctx* c, const pm_graph* g, const pm_plan* const
   a.root_reads = o.root_reads;
   a.root_order = o.root_order;
   a.timeout_ns = (unsigned long long)(o.timeout_ms > 0 ? o.timeout_ms : 600000) * 1000000ull;
+  for (int i = 0; i < nplans; i++) a.plans[i] = L->dp[i];
   L->active0 = (unsigned int)L->warps;
   if (L->paged) {
     st = paged_prepare(c, const_cast<pm_graph*>(g), L->cold, &a.pg);
@@ -1967,17 +1977,16 @@ static pm_status setup_launch(pm_ctx* c, const pm_graph* g, const pm_plan* const
   return PM_OK;
 }
 
-// Enqueues one launch on the context stream: plan upload, control reset,
-// the persistent kernel between events eb/ee, and the read-back of counts,
-// stats and status into host_ctl.  Capturable into a CUDA graph (host_ctl,
-// dp_src and active_src must then be pinned).
-static pm_status enqueue_launch(pm_ctx* c, Launch& L, const DPlan* dp_src, const unsigned int* active_src,
+// Enqueues one launch on the context stream: control reset, the persistent
+// kernel (its plans travel in its parameter block) between events eb/ee, and
+// the read-back of counts, stats and status into host_ctl.  Capturable into a
+// CUDA graph (host_ctl and active_src must then be pinned).
+static pm_status enqueue_launch(pm_ctx* c, Launch& L, const unsigned int* active_src,
                                 unsigned long long* host_ctl, cudaEvent_t eb, cudaEvent_t ee) {
-  CK(cudaMemcpyToSymbolAsync(c_plans, dp_src, sizeof(DPlan) * L.nplans, 0, cudaMemcpyHostToDevice, c->stream));
   CK(cudaMemsetAsync(L.a.cursors, 0, L.ctl_words * 8, c->stream));
   CK(cudaMemcpyAsync(L.a.active, active_src, sizeof(unsigned int), cudaMemcpyHostToDevice, c->stream));
   if (eb) CK(cudaEventRecord(eb, c->stream));
-  (void)cudaGetLastError();  // drop a stale error from an earlier call
+  PM_CK_PENDING("pm_match");
   L.kfn<<<L.blocks, L.threads, L.smem, c->stream>>>(L.a);
   CK(cudaGetLastError());
   if (ee) CK(cudaEventRecord(ee, c->stream));
@@ -2056,7 +2065,7 @@ extern "C" pm_status pm_match(pm_ctx* c, const pm_graph* g, const pm_plan* const
   c->h_active = L->active0;
   unsigned long long host_ctl[kCtlRead];
   pm_stats pst;
-  st = run_launch(c, g, *L, [&]() { return enqueue_launch(c, *L, L->dp, &c->h_active, host_ctl, e1, e2); }, &pst);
+  st = run_launch(c, g, *L, [&]() { return enqueue_launch(c, *L, &c->h_active, host_ctl, e1, e2); }, &pst);
   if (st != PM_OK) return st;
   float kms = 0, rms = 0;
   CK(cudaEventElapsedTime(&kms, e1, e2));
@@ -2078,7 +2087,6 @@ struct pm_query {
   size_t arena_bytes = 0;
   unsigned long long* d_ctl = nullptr;
   size_t ctl_bytes = 0;
-  DPlan* h_dp = nullptr;              // pinned
   unsigned int* h_active = nullptr;   // pinned
   unsigned long long* h_ctl = nullptr;  // pinned
   cudaEvent_t eb = nullptr, ee = nullptr;
@@ -2097,7 +2105,6 @@ extern "C" void pm_query_free(pm_query* q) {
   free_dev(q->d_roots);
   free_dev(q->d_arena);
   free_dev(q->d_ctl);
-  if (q->h_dp) cudaFreeHost(q->h_dp);
   if (q->h_active) cudaFreeHost(q->h_active);
   if (q->h_ctl) cudaFreeHost(q->h_ctl);
   delete q;
@@ -2120,16 +2127,14 @@ extern "C" pm_status pm_query_prepare(pm_ctx* c, const pm_graph* g, const pm_pla
   CK(cudaEventRecord(c->ev[1], c->stream));
   CK(cudaEventSynchronize(c->ev[1]));
   CK(cudaEventElapsedTime(&q->roots_ms, c->ev[0], c->ev[1]));
-  CK(cudaMallocHost(&q->h_dp, sizeof(DPlan) * PM_MAX_BATCH));
   CK(cudaMallocHost(&q->h_active, sizeof(unsigned int)));
   CK(cudaMallocHost(&q->h_ctl, sizeof(unsigned long long) * kCtlRead));
-  memcpy(q->h_dp, q->L.dp, sizeof(DPlan) * q->L.nplans);
   *q->h_active = q->L.active0;
   CK(cudaEventCreate(&q->eb));
   CK(cudaEventCreate(&q->ee));
   CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
   // timing events stay outside the graph (recorded around each replay)
-  pm_status est = enqueue_launch(c, q->L, q->h_dp, q->h_active, q->h_ctl, nullptr, nullptr);
+  pm_status est = enqueue_launch(c, q->L, q->h_active, q->h_ctl, nullptr, nullptr);
   cudaError_t cerr = cudaStreamEndCapture(c->stream, &q->graph);
   if (est != PM_OK) return est;
   CK(cerr);
@@ -2163,15 +2168,15 @@ extern "C" pm_status pm_query_run(pm_query* q, uint64_t* counts_out, pm_stats* s
 // ---------------------------------------------------------------------
 // Allocation-free entry point: pm_match_static.
 //
-// For callers that must not allocate device memory -- code running where
-// cudaMalloc is not allowed or not wanted: inside a host callback, in a
-// process whose allocator is owned by another framework with a fixed pool,
-// in a real-time service that has budgeted every byte up front, or while
-// another library holds the device allocator lock.  The caller provides the
-// graph arrays and receives the count; everything the launch needs besides
-// them (control block, donation ring, root list, per-warp arenas) lives in
-// one file-scope device array of PM_STATIC_SCRATCH_BYTES that each GPU keeps
-// from module load until the process exits.
+// For callers that must not allocate device memory -- code running while
+// another library holds the device allocator lock, in a process whose
+// allocator is owned by a framework with a fixed pool, or in a service that
+// has budgeted every byte up front.  The caller provides the graph arrays
+// and receives the count; everything the launch needs besides them (control
+// block, donation ring, root list, per-warp arenas) lives in one file-scope
+// device array of PM_STATIC_SCRATCH_BYTES that each GPU keeps from module
+// load until the process exits.  The plan travels in the kernel's parameter
+// block like every launch's, so the scratch is the only state it shares.
 // ---------------------------------------------------------------------
 static __device__ __align__(256) unsigned char g_static_scratch[PM_STATIC_SCRATCH_BYTES];
 
@@ -2233,6 +2238,7 @@ extern "C" pm_status pm_match_static(const uint64_t* d_rowptr, const int32_t* d_
                                      pm_stats* stats_out) {
   if (!d_rowptr || (nadj > 0 && !d_colidx) || !plan || !count_out || n < 0 || max_degree < 0)
     return fail(PM_ERR_INVALID, "pm_match_static: bad arguments");
+  if (n > INT32_MAX - 1) return fail(PM_ERR_INVALID, "pm_match_static: %lld vertices exceed int32 ids", (long long)n);
   const Plan& p = *plan_of(plan);
   if (p.labeled && !d_labels) return fail(PM_ERR_INVALID, "pm_match_static: labeled plan without labels");
   pm_run_opts o;
@@ -2283,7 +2289,7 @@ extern "C" pm_status pm_match_static(const uint64_t* d_rowptr, const int32_t* d_
 
   CK(cudaMemsetAsync(base, 0, ctl_bytes + 64, st));  // previous calls leave their contents behind
   const RootFilter f = to_filter(p);
-  (void)cudaGetLastError();  // drop a stale error from an earlier call
+  PM_CK_PENDING("pm_match_static");
   roots_static_kernel<<<4 * nsm, 256, 0, st>>>(d_rowptr, d_colidx, d_labels, n, f, roots, root_cap, rcount);
   CK(cudaGetLastError());
   unsigned long long nroots = 0;
@@ -2295,9 +2301,19 @@ extern "C" pm_status pm_match_static(const uint64_t* d_rowptr, const int32_t* d_
   const size_t roots_bytes = ((size_t)nroots * sizeof(int2) + 255) & ~(size_t)255;
   int32_t* arena = (int32_t*)((unsigned char*)roots + roots_bytes);
   const size_t arena_bytes = after_ctl - roots_bytes;
+  // kernel variant by register cap, as pm_match chooses it
+  int variant = o.high_occupancy;
+  if (variant == 0) variant = (wpb <= 8) ? 2 : 3;
+  if (variant < 0 || variant > 3) return fail(PM_ERR_INVALID, "pm_match_static: high_occupancy must be 0..3");
+  if ((variant == 1 || variant == 2) && wpb > 8)
+    return fail(PM_ERR_INVALID, "pm_match_static: warps_per_block 16 needs the uncapped kernel variant");
+  void (*kfn)(const MatchArgs) =
+      variant == 1 ? (p.labeled ? match_kernel<true, false, 4> : match_kernel<false, false, 4>)
+      : variant == 2 ? (p.labeled ? match_kernel<true, false, 3> : match_kernel<false, false, 3>)
+                     : (p.labeled ? match_kernel<true, false, 1> : match_kernel<false, false, 1>);
   int per_sm = 0;
-  auto kfn = p.labeled ? match_kernel<true, false, 1> : match_kernel<false, false, 1>;
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, wpb * 32, sizeof(WarpState) * wpb));
+  if (o.blocks_per_sm > 0) per_sm = std::min(per_sm, o.blocks_per_sm);
   int64_t blocks = std::max(1, per_sm) * (int64_t)nsm;
   blocks = std::min<int64_t>(blocks, (int64_t)(arena_bytes / ((size_t)wpb * warp_bytes)));
   if (blocks < 1) return fail(PM_ERR_INTERNAL, "pm_match_static: no room for a block of arenas");
@@ -2305,12 +2321,14 @@ extern "C" pm_status pm_match_static(const uint64_t* d_rowptr, const int32_t* d_
   DPlan dp = to_dplan(p);
   dp.roots = roots;
   dp.nroots = (int64_t)nroots;
-  CK(cudaMemcpyToSymbolAsync(c_plans, &dp, sizeof(DPlan), 0, cudaMemcpyHostToDevice, st));
   MatchArgs a;
   memset(&a, 0, sizeof(a));
+  a.plans[0] = dp;
   a.rowptr = d_rowptr;
   a.colidx = d_colidx;
   a.labels = d_labels;
+  a.leaf_flat = o.leaf_per_lane ? 0 : 1;
+  a.lane_subtree_max = lane_subtree_limit(o);
   a.n = (int32_t)n;
   a.nplans = 1;
   a.T = T;
@@ -2339,7 +2357,7 @@ extern "C" pm_status pm_match_static(const uint64_t* d_rowptr, const int32_t* d_
   a.timeout_ns = (unsigned long long)(o.timeout_ms > 0 ? o.timeout_ms : 600000) * 1000000ull;
   const unsigned int active0 = (unsigned int)warps;
   CK(cudaMemcpyAsync(a.active, &active0, sizeof(active0), cudaMemcpyHostToDevice, st));
-  (void)cudaGetLastError();  // drop a stale error from an earlier call
+  PM_CK_PENDING("pm_match_static");
   kfn<<<(int)blocks, wpb * 32, sizeof(WarpState) * wpb, st>>>(a);
   CK(cudaGetLastError());
   unsigned long long host_ctl[kCtlRead];

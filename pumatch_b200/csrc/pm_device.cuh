@@ -70,7 +70,25 @@ enum : int32_t { PAGE_ABSENT = -1, PAGE_LOADING = -2 };
 
 struct PagedState;  // host-side page service state (pm_paging.cu)
 
+// Called before a launch: an error still pending from an earlier call (this
+// library's or another's on the same thread) is reported, not silently
+// cleared, so the launch's own check afterwards sees only its own error.
+// cudaErrorNotReady is a query status, not a failure, and is just cleared.
+inline pm_status pending_error(const char* where) {
+  const cudaError_t e = cudaPeekAtLastError();
+  if (e == cudaSuccess) return PM_OK;
+  (void)cudaGetLastError();
+  if (e == cudaErrorNotReady) return PM_OK;
+  return fail(PM_ERR_CUDA, "%s: an earlier CUDA call left an error pending: %s", where, cudaGetErrorString(e));
+}
+
 }  // namespace pm
+
+#define PM_CK_PENDING(where)                           \
+  do {                                                 \
+    const pm_status s_ = pm::pending_error(where);     \
+    if (s_ != PM_OK) return s_;                        \
+  } while (0)
 
 // Opaque handles of the C-ABI (pumatch.h), shared by the device TUs.
 struct pm_graph {

@@ -671,16 +671,8 @@ extern "C" pm_status pm_gen_rmat(int64_t n, int64_t m, double a, double b, doubl
   const uint32_t tc = (uint32_t)std::lround((a + b + c) * 65536.0);
   std::vector<uint64_t> keys = sample_unique(m, seed, [&](Rng& r, uint64_t* out, int64_t cnt) {
     for (int64_t k = 0; k < cnt; k++) {
-      uint64_t u = 0, v = 0, bits = 0;
-      for (int l = 0; l < scale; l++) {
-        if ((l & 3) == 0) bits = r.next();
-        const uint32_t x = (uint32_t)(bits & 0xffff);
-        bits >>= 16;
-        const uint32_t bu = x >= tb, bv = (x >= ta && x < tb) || x >= tc;
-        u = (u << 1) | bu;
-        v = (v << 1) | bv;
-      }
-      out[k] = (u >= (uint64_t)n || v >= (uint64_t)n || u == v) ? UINT64_MAX : edge_key((uint32_t)u, (uint32_t)v);
+      uint32_t u, v;
+      out[k] = rmat_draw(r, scale, (uint64_t)n, ta, tb, tc, &u, &v) ? edge_key(u, v) : UINT64_MAX;
     }
   });
   if ((int64_t)keys.size() != m) return fail(PM_ERR_INVALID, "pm_gen_rmat: could not reach %lld edges", (long long)m);

@@ -339,7 +339,7 @@ extern "C" pm_status pm_mlp_create(int device, uint64_t seed, pm_mlp** out) {
   CKL(cudaMemcpy(m->w, h.data(), sizeof(float) * NPARAM, cudaMemcpyHostToDevice));
   CKL(cudaMemset(m->m, 0, sizeof(float) * NPARAM));
   CKL(cudaMemset(m->v, 0, sizeof(float) * NPARAM));
-  (void)cudaGetLastError();  // drop a stale error from an earlier call
+  PM_CK_PENDING("pm_mlp_create");
   quantize_kernel<<<(NPARAM + 255) / 256, 256>>>(m->w, m->wq);
   CKL(cudaGetLastError());
   CKL(cudaDeviceSynchronize());
@@ -358,7 +358,7 @@ extern "C" pm_status pm_mlp_set_weights(pm_mlp* m, const float* host_in) {
   if (!m || !host_in) return fail(PM_ERR_INVALID, "pm_mlp_set_weights: null argument");
   CKL(cudaSetDevice(m->device));
   CKL(cudaMemcpy(m->w, host_in, sizeof(float) * NPARAM, cudaMemcpyHostToDevice));
-  (void)cudaGetLastError();  // drop a stale error from an earlier call
+  PM_CK_PENDING("pm_mlp_set_weights");
   quantize_kernel<<<(NPARAM + 255) / 256, 256>>>(m->w, m->wq);
   CKL(cudaGetLastError());
   CKL(cudaDeviceSynchronize());
@@ -373,7 +373,7 @@ extern "C" pm_status pm_mlp_forward(pm_mlp* m, const float* d_x, int64_t n, floa
   CKL(cudaSetDevice(m->device));
   if (n == 0) return PM_OK;
   const int blocks = (int)std::min<int64_t>((n + 127) / 128, 8 * m->nsm);
-  (void)cudaGetLastError();  // drop a stale error from an earlier call
+  PM_CK_PENDING("MLP kernels");
   mlp_forward_kernel<<<blocks, 128>>>(m->wq, d_x, n, d_y);
   CKL(cudaGetLastError());
   CKL(cudaDeviceSynchronize());
@@ -389,7 +389,7 @@ extern "C" pm_status pm_mlp_gradient(pm_mlp* m, const float* d_x, const float* d
   const int blocks = (int)std::min<int64_t>((n + TILE - 1) / TILE, 2 * m->nsm);
   CKL(cudaFuncSetAttribute(mlp_backward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)sizeof(BackwardSmem)));
-  (void)cudaGetLastError();  // drop a stale error from an earlier call
+  PM_CK_PENDING("MLP kernels");
   mlp_backward_kernel<<<blocks, 256, sizeof(BackwardSmem)>>>(m->wq, d_x, d_t, n, m->g, m->loss);
   CKL(cudaGetLastError());
   if (host_grad) CKL(cudaMemcpy(host_grad, m->g, sizeof(float) * NPARAM, cudaMemcpyDeviceToHost));
@@ -405,7 +405,7 @@ extern "C" pm_status pm_mlp_train_step(pm_mlp* m, const float* d_x, const float*
   m->step++;
   const float b1 = 0.9f, b2 = 0.999f;
   const float c1 = 1.f - std::pow(b1, (float)m->step), c2 = 1.f - std::pow(b2, (float)m->step);
-  (void)cudaGetLastError();  // drop a stale error from an earlier call
+  PM_CK_PENDING("MLP kernels");
   adam_kernel<<<(NPARAM + 255) / 256, 256>>>(m->w, m->wq, m->g, m->m, m->v, lr, b1, b2, 1e-8f, c1, c2);
   CKL(cudaGetLastError());
   CKL(cudaDeviceSynchronize());
@@ -430,24 +430,33 @@ extern "C" pm_status pm_root_features(pm_ctx* c, const pm_graph* g, const pm_pla
   // degree-quantile table
   unsigned int* hist = nullptr;
   float* rank = nullptr;
+  PM_CK_PENDING("pm_root_features");
   CKL(cudaMalloc(&hist, 256 * sizeof(unsigned int)));
   CKL(cudaMalloc(&rank, sizeof(float) * std::max<int64_t>(g->n, 1)));
   CKL(cudaMemset(hist, 0, 256 * sizeof(unsigned int)));
-  (void)cudaGetLastError();  // drop a stale error from an earlier call
   deg_hist_kernel<<<1024, 256>>>(g->d_rowptr, g->n, hist);
   std::vector<unsigned int> h(256);
-  CKL(cudaMemcpy(h.data(), hist, 256 * sizeof(unsigned int), cudaMemcpyDeviceToHost));
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpy(h.data(), hist, 256 * sizeof(unsigned int), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) {
+    cudaFree(hist);
+    cudaFree(rank);
+    CKL(e);
+  }
   unsigned int acc = 0;
   for (int i = 0; i < 256; i++) { acc += h[i]; h[i] = acc; }
-  CKL(cudaMemcpy(hist, h.data(), 256 * sizeof(unsigned int), cudaMemcpyHostToDevice));
-  (void)cudaGetLastError();  // drop a stale error from an earlier call
-  deg_rank_kernel<<<1024, 256>>>(g->d_rowptr, g->n, hist, g->maxdeg, rank);
+  e = cudaMemcpy(hist, h.data(), 256 * sizeof(unsigned int), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    deg_rank_kernel<<<1024, 256>>>(g->d_rowptr, g->n, hist, g->maxdeg, rank);
+    e = cudaGetLastError();
+  }
   const Plan* pl = plan_of(p);
   const int32_t* colidx = g->residency == PM_RESIDENT_HBM ? g->d_colidx : g->h_colidx_dev;
-  (void)cudaGetLastError();  // drop a stale error from an earlier call
-  features_kernel<<<4 * c->nsm, 256>>>(g->d_rowptr, colidx, g->d_labels, g->d_maxnbrdeg, rank, g->nlabels,
-                                       pl->nnodes > 2 ? pl->vertex_label[2] : 0, roots, n, d_features);
-  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) {
+    features_kernel<<<4 * c->nsm, 256>>>(g->d_rowptr, colidx, g->d_labels, g->d_maxnbrdeg, rank, g->nlabels,
+                                         pl->nnodes > 2 ? pl->vertex_label[2] : 0, roots, n, d_features);
+    e = cudaGetLastError();
+  }
   cudaError_t s2 = cudaDeviceSynchronize();
   cudaFree(hist);
   cudaFree(rank);

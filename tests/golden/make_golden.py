@@ -4,7 +4,7 @@ Run in a container that has the reference sources (the recipe oracle/Makefile
 `make ref` compiles the reference's own, untouched host headers into
 oracle/_ref/):
 
-    make -C oracle ref && python tests/golden/make_golden.py
+    PM_REF_DIR=<reference checkout> make -C oracle ref && python tests/golden/make_golden.py
 
 Writes
   graphs/<name>.{meta.txt,vertex.bin,edge.bin,label.bin}  seeded small graphs

@@ -1,0 +1,129 @@
+"""Writes tests/golden/root_samples.json: seeded root samples of the configured
+queries whose whole root lists no exact enumerator can finish, with the
+oracle's exact per-root counts.
+
+    python tests/golden/make_root_samples.py [--threads N] [--only NAME]
+
+A sample walks a seeded permutation of the query's root list (reference
+order, the positions the library's root ids use) and keeps each root whose
+Knuth estimate of set operations is at most `budget`, until the kept roots'
+estimates sum to `budget`: a fixed-size unit of work per bench step, drawn at
+random from all roots but the ones heavier than a whole step.  Every kept
+root is then counted exactly by the oracle (each root's DFS divided over
+threads at level 1, the same DFS per piece), giving the raw count, the final
+count (x |Aut| when unlabeled) and the set operations, which the GPU's
+per-root counts and launch statistics must equal.
+
+The graph is built by the oracle's generator (the workload definition the
+product's generator implements; a CPU test pins the two equal), and its
+arrays' sha256 is stored so a run on another machine can check it has the
+same graph.
+"""
+from __future__ import annotations
+
+import argparse
+import hashlib
+import json
+import os
+import sys
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+sys.path.insert(0, ROOT)
+
+import pm_oracle as orc  # noqa: E402
+from pumatch_b200 import patterns as P  # noqa: E402
+
+# the configured C1 query: Chung-Lu 100K vertices / 1M edges (gamma 2.1,
+# i0 10, expected degrees capped at 5,000, seed 1), unlabeled 7-cycle
+SAMPLES = {
+    "chunglu100k_c7": dict(graph=dict(kind="chung_lu", n=100_000, m=1_000_000, gamma=2.1, i0=10.0, max_w=5000.0,
+                                      seed=1),
+                           labeled=False, pattern=P.to_g(*P.cycle(7)), perm_seed=7, budget=5e9,
+                           est_probes=400, est_seed=11),
+}
+
+
+def build_graph(gd):
+    if gd["kind"] == "chung_lu":
+        return orc.gen_chung_lu(gd["n"], gd["m"], gd["gamma"], gd["i0"], gd["max_w"], gd["seed"])
+    return orc.gen_rmat(gd["n"], gd["m"], gd["a"], gd["b"], gd["c"], gd["seed"])
+
+
+def graph_digest(rowptr: np.ndarray, colidx: np.ndarray) -> str:
+    h = hashlib.sha256()
+    h.update(np.ascontiguousarray(rowptr, dtype=np.uint64).tobytes())
+    h.update(np.ascontiguousarray(colidx, dtype=np.int32).tobytes())
+    return h.hexdigest()
+
+
+def choose(g, p, roots, spec):
+    perm = np.random.default_rng(spec["perm_seed"]).permutation(len(roots))
+    kept, total, looked = [], 0.0, 0
+    for i in perm:
+        looked += 1
+        so, _, _ = orc.estimate(g, p, roots[i:i + 1], probes=spec["est_probes"], seed=spec["est_seed"])
+        if so > spec["budget"]:
+            continue
+        kept.append((int(i), so))
+        total += so
+        if total >= spec["budget"]:
+            break
+    return kept, looked
+
+
+def make(name, threads):
+    spec = SAMPLES[name]
+    rp, ci = build_graph(spec["graph"])
+    g = orc.Graph(rp, ci, None)
+    p = orc.plan(spec["pattern"], spec["labeled"])
+    roots = orc.roots(g, p)
+    kept, looked = choose(g, p, roots, spec)
+    idx = np.array([i for i, _ in kept], dtype=np.int64)
+    t0 = time.time()
+    total, per_root, done, pieces, st = orc.count_split(g, p, roots[idx], threads=threads)
+    assert done == pieces
+    mult = 1 if spec["labeled"] else p.multiplicity
+    so_total, _, _ = orc.estimate(g, p, roots, probes=20000, seed=spec["est_seed"])
+    rec = {
+        "graph": spec["graph"], "graph_sha256": graph_digest(rp, ci), "n_adj": int(len(ci)),
+        "labeled": spec["labeled"], "pattern": spec["pattern"], "multiplicity": int(mult),
+        "rule": (f"seeded permutation (numpy default_rng({spec['perm_seed']})) of the {len(roots)} root edges; "
+                 f"keep roots whose Knuth estimate ({spec['est_probes']} probes, seed {spec['est_seed']}) is at "
+                 f"most {spec['budget']:.0e} set operations until the kept estimates sum to {spec['budget']:.0e}"),
+        "n_roots_total": int(len(roots)), "roots_examined": looked,
+        "query_set_ops_estimate": so_total,
+        "roots": [{"index": int(i), "v0": int(roots[i][0]), "v1": int(roots[i][1]), "raw_count": int(c),
+                   "count": int(c) * mult, "set_ops_estimate": so}
+                  for (i, so), c in zip(kept, per_root)],
+        "raw_count": int(total), "count": int(total) * mult, "set_ops": int(st["set_ops"]),
+        "alg_bytes": int(st["alg_bytes"]), "oracle_s": round(time.time() - t0, 1), "oracle_threads": threads,
+    }
+    return rec
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--threads", type=int, default=os.cpu_count() or 1)
+    ap.add_argument("--only", default=None)
+    ap.add_argument("--out", default=os.path.join(HERE, "root_samples.json"))
+    args = ap.parse_args()
+    out = {}
+    if os.path.exists(args.out):
+        with open(args.out) as f:
+            out = json.load(f)
+    for name in SAMPLES:
+        if args.only and name != args.only:
+            continue
+        out[name] = make(name, args.threads)
+        print(name, out[name]["count"], out[name]["set_ops"], out[name]["oracle_s"], "s", flush=True)
+        with open(args.out, "w") as f:
+            json.dump(out, f, indent=1)
+
+
+if __name__ == "__main__":
+    main()

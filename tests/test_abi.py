@@ -89,6 +89,21 @@ def test_no_cpu_fallback():
         os.remove(pat)
 
 
+def test_static_entry_argument_checks():
+    """pm_match_static refuses, before touching a device, what it cannot run:
+    vertex ids beyond int32 and the per-root options it does not support."""
+    import ctypes as C
+    from pumatch_b200 import patterns as P
+    plan = pm.PatternPreprocessor(text=P.to_g(*P.cycle(4)), labeled=False)
+    fake = C.c_void_p(16)  # never dereferenced: the checks come first
+    cnt = C.c_uint64()
+    rc = pm.lib().pm_match_static(fake, fake, None, 1 << 31, 10, 4, plan._h, None, None, C.byref(cnt), None)
+    assert rc == pm.PM_ERR_INVALID and b"int32" in pm.lib().pm_last_error()
+    o = pm.Context._opts(root_counts_ptr=16)
+    rc = pm.lib().pm_match_static(fake, fake, None, 100, 10, 4, plan._h, C.byref(o), None, C.byref(cnt), None)
+    assert rc == pm.PM_ERR_INVALID
+
+
 def test_cli_usage():
     r = subprocess.run([pm.CLI_PATH], capture_output=True, text=True)
     assert r.returncode == 2 and "usage" in r.stderr
@@ -148,7 +163,7 @@ int main(void){
 
 
 def test_c_program_links_and_runs_host_entry_points(tmp_path):
-    """A plain C caller, as INTEGRATION.md's snippet: compile a pattern,
+    """A plain C caller that only includes pumatch.h: compile a pattern,
     describe it, build and renumber a graph, and get PM_ERR_NO_DEVICE (not a
     CPU fallback) from the device entry points."""
     src = r'''

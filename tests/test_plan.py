@@ -65,15 +65,17 @@ def test_bad_pattern_text():
     assert e.value.status == pm.PM_ERR_IO
 
 
-REF_PAT = sorted(glob.glob("/root/reference/pattern/*.g"))
+# the reference checkout, when one is named (PM_REF_DIR); skipped otherwise
+REF_DIR = os.environ.get("PM_REF_DIR", "")
+REF_PAT = sorted(glob.glob(os.path.join(REF_DIR, "pattern", "*.g"))) if REF_DIR else []
 REF_PROBE = os.path.join(os.path.dirname(os.path.dirname(__file__)), "oracle", "_ref")
 
 
 @pytest.mark.skipif(not REF_PAT or not os.path.exists(os.path.join(REF_PROBE, "ref_plan_dump_labeled")),
-                    reason="reference sources / probe not present")
+                    reason="PM_REF_DIR unset, or the reference-built probe is missing")
 @pytest.mark.parametrize("path", REF_PAT, ids=os.path.basename)
 def test_reference_pattern_files(path):
-    """The reference's own 20 pattern files, where the reference is mounted."""
+    """The reference's own 20 pattern files, where a reference checkout is named."""
     for mode in ("labeled", "unlabeled"):
         ref = json.loads(subprocess.run([os.path.join(REF_PROBE, f"ref_plan_dump_{mode}"), path],
                                         capture_output=True, text=True, check=True).stdout)

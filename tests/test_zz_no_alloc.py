@@ -1,8 +1,9 @@
 """The allocation-free entry point, pm_match_static, against pm_match.
 
-pm_match_static serves callers that cannot allocate device memory (a host
-callback, a service that owns a fixed memory budget, a framework that owns the
-allocator): its scratch is one file-scope device array of a fixed size.  The
+pm_match_static serves callers that cannot allocate device memory (code that
+runs while another library holds the allocator lock, a service that owns a
+fixed memory budget, a framework that owns the allocator): its scratch is one
+file-scope device array of a fixed size.  The
 test calls it through the C-ABI twice in a row -- the second call finds the
 first call's leftovers in the shared scratch -- and compares each result with
 the allocating entry point on the same inputs (counts are integers: equal).
@@ -60,6 +61,13 @@ def test_static_entry_matches_allocating_entry(labeled):
             assert rc == pm.PM_OK, pm.lib().pm_last_error()
             assert got == want[0]
             assert st["set_ops"] == wst["set_ops"] and st["alg_bytes"] == wst["alg_bytes"]
+        # the launch options mean what they mean for pm_match
+        for kw in (dict(leaf_per_lane=1), dict(lane_subtree_max=-1), dict(high_occupancy=3, warps_per_block=16),
+                   dict(high_occupancy=1, blocks_per_sm=1)):
+            w2, _ = ctx.match(g, [p], **kw)
+            rc, got, _ = _static(arrays, p, **kw)
+            assert rc == pm.PM_OK, pm.lib().pm_last_error()
+            assert got == w2[0] == want[0], kw
     g.close()
     ctx.close()
 
