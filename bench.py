@@ -52,6 +52,10 @@ from pumatch_b200 import patterns as P  # noqa: E402
 _CL100K = dict(kind="chung_lu", n=100_000, m=1_000_000, gamma=2.1, i0=10.0, max_w=5000.0, seed=1)
 _RMAT1M = dict(kind="rmat", n=1 << 20, m=16 << 20, a=0.57, b=0.19, c=0.19, seed=2)
 _RMAT128K = dict(kind="rmat", n=1 << 17, m=16 << 17, a=0.57, b=0.19, c=0.19, seed=2)
+# the configured R-MAT graph: 65M vertices, 1.8e9 undirected edges (3.6e9
+# adjacency entries, 14.4 GB), generated on the GPU (same arrays as the host
+# generator)
+_RMAT65M = dict(kind="rmat", n=65_000_000, m=1_800_000_000, a=0.57, b=0.19, c=0.19, seed=2, device=0)
 WORKLOADS = {
     # the configured small query: Chung-Lu 100K vertices / 1M edges, gamma
     # 2.1, expected degrees capped at 5,000, unlabeled, in HBM; the 7-cycle,
@@ -79,6 +83,15 @@ WORKLOADS = {
     "rmat1m_c5t2_lab32_paged": dict(graph=_RMAT1M, labeled=True, n_labels=32, label_seed=102,
                                     pattern_label_seed=202, patterns=[("C5t2", P.cycle_tail(5, 2))],
                                     paged=dict(frame_fraction=0.88, static_fraction=0.6, page_bytes=64 << 10)),
+    # the configured R-MAT query: 8 uniform labels, the 5-cycle plus a 2-vertex
+    # pendant path (labels from the 8), on a seeded root sample; paged through
+    # a 4 GB frame pool of 64 KB pages (the whole adjacency stays in pinned
+    # host memory), and in HBM for the set-operation roofline
+    "rmat65m_c5t2_lab8_paged": dict(graph=_RMAT65M, labeled=True, n_labels=8, label_seed=102, pattern_label_seed=202,
+                                    patterns=[("C5t2", P.cycle_tail(5, 2))], sample="rmat65m_c5t2_lab8",
+                                    paged=dict(frame_bytes=4 << 30, static_bytes=0, page_bytes=64 << 10)),
+    "rmat65m_c5t2_lab8": dict(graph=_RMAT65M, labeled=True, n_labels=8, label_seed=102, pattern_label_seed=202,
+                              patterns=[("C5t2", P.cycle_tail(5, 2))], sample="rmat65m_c5t2_lab8"),
     # twenty seeded 4-7-vertex patterns in one persistent launch
     "rmat128k_batch20_lab32": dict(graph=_RMAT128K, labeled=True, n_labels=32, label_seed=102, batch_seed=303),
     # learned-scheduler comparison (--learned): trained on seeds 11, 12, 13
@@ -111,7 +124,7 @@ def make_graph(g, seed=None, via_oracle=False):
         return pm.HostGraph(rp, ci)
     if g["kind"] == "chung_lu":
         return pm.gen_chung_lu(g["n"], g["m"], gamma=g["gamma"], i0=g["i0"], max_w=g["max_w"], seed=seed)
-    return pm.gen_rmat(g["n"], g["m"], a=g["a"], b=g["b"], c=g["c"], seed=seed)
+    return pm.gen_rmat(g["n"], g["m"], a=g["a"], b=g["b"], c=g["c"], seed=seed, device=g.get("device"))
 
 
 def build_workload(name, graph_seed=None, via_oracle=False):
@@ -162,8 +175,11 @@ def place_graph(w, hg, device):
     if not pg:
         return pm.GraphPreprocessor.from_host(hg, labeled=w["labeled"], device=device)
     pb = pg["page_bytes"]
-    pool = max(pb, int(hg.colidx.nbytes * pg["frame_fraction"]) // pb * pb)
-    static = int(hg.colidx.nbytes * pg.get("static_fraction", 0.0)) // pb * pb
+    if "frame_bytes" in pg:  # an absolute pool (the configured 4 GB)
+        pool, static = pg["frame_bytes"] // pb * pb, pg.get("static_bytes", 0) // pb * pb
+    else:  # a share of the adjacency array
+        pool = max(pb, int(hg.colidx.nbytes * pg["frame_fraction"]) // pb * pb)
+        static = int(hg.colidx.nbytes * pg.get("static_fraction", 0.0)) // pb * pb
     return pm.GraphPreprocessor.from_host(hg, labeled=w["labeled"], device=device, paged=True,
                                           page_bytes=pb, frame_pool_bytes=pool, static_pool_bytes=static)
 
@@ -254,8 +270,8 @@ def cpu_measure(hg, texts, labeled, threads, sample=None, time_limit_s=15.0, see
     """Times the oracle on the host cores.
 
     With a root sample: the sampled roots' DFS pieces (level-1 candidates) in
-    a seeded shuffled order, stopped at time_limit_s; the rate is matches per
-    second over the pieces done.  Without one: seeded random root samples,
+    a seeded shuffled order, stopped at time_limit_s (inside a piece too);
+    the rate is the matches found per second.  Without one: seeded random root samples,
     grown until a run takes about a quarter of time_limit_s; with per_root the
     per-root counts of the last sample are returned for the parity check.
     Returns dict(matches, seconds, sample text[, roots, per_root])."""
@@ -271,8 +287,8 @@ def cpu_measure(hg, texts, labeled, threads, sample=None, time_limit_s=15.0, see
                                              shuffle_seed=seed)
         dt = time.perf_counter() - t0
         return {"matches": c * mult[0], "seconds": dt,
-                "sample": f"{done} of the {tot} level-1 pieces of the {len(rts)} sampled root edges (seeded "
-                          f"shuffled order), {dt:.1f} s on {threads} threads"}
+                "sample": f"the {len(rts)} sampled root edges' DFS split into {tot} level-1 pieces, taken in a "
+                          f"seeded shuffled order for {dt:.1f} s on {threads} threads ({done} pieces finished)"}
     rng = np.random.default_rng(seed)
     roots = [orc.roots(g, p) for p in plans]
     total_roots = sum(len(r) for r in roots)
@@ -347,6 +363,14 @@ def run_ours(args, workload):
                                 device_id=torch.device("cuda", local))
     w, hg, texts = build_workload(workload)
     sample = load_sample(w, hg)
+    subset = False
+    if sample is not None and args.sample_roots:
+        # profiling a part of the sample: its roots' counts are still checked
+        keep = [int(x) for x in args.sample_roots.split(",")]
+        sample = dict(sample, roots=[sample["roots"][i] for i in keep])
+        sample["raw_count"] = sum(r["raw_count"] for r in sample["roots"])
+        sample["count"] = sum(r["count"] for r in sample["roots"])
+        subset = True
     labeled = w["labeled"]
     plans = [pm.PatternPreprocessor(text=t, labeled=labeled) for _, t in texts]
     ctx = pm.Context(local)
@@ -434,7 +458,8 @@ def run_ours(args, workload):
     d2h = 8 * len(plans)
     if order_h is not None:
         h2d += order_h.numel() * 4
-    for k in range(max(1, min(args.steps, 3))):
+    e2e_steps = 1 if hg.colidx.nbytes > (1 << 30) else max(1, min(args.steps, 3))
+    for k in range(e2e_steps):
         torch.cuda.synchronize()
         if dist:
             dist.barrier()
@@ -471,12 +496,13 @@ def run_ours(args, workload):
         if sample is not None:
             # every sampled root against the oracle's exact per-root count
             bad = [r["index"] for r in sample["roots"] if int(per_root_gpu[r["index"]]) != r["raw_count"]]
-            ok = (not bad and counts_total[0] == sample["count"] and set_ops // args.steps == sample["set_ops"]
-                  and alg_bytes // args.steps == sample["alg_bytes"])
+            ok = (not bad and counts_total[0] == sample["count"] and
+                  (subset or (set_ops // args.steps == sample["set_ops"] and
+                              alg_bytes // args.steps == sample["alg_bytes"])))
             parity = {"roots_checked": len(sample["roots"]), "ok": ok, "mismatched_roots": bad,
                       "count": counts_total[0], "oracle_count": sample["count"],
-                      "set_ops_equal": set_ops // args.steps == sample["set_ops"],
-                      "alg_bytes_equal": alg_bytes // args.steps == sample["alg_bytes"],
+                      "set_ops_equal": None if subset else set_ops // args.steps == sample["set_ops"],
+                      "alg_bytes_equal": None if subset else alg_bytes // args.steps == sample["alg_bytes"],
                       "against": "oracle exact per-root counts, set operations and algorithmic bytes "
                                  "(tests/golden/root_samples.json)"}
         line = {
@@ -506,6 +532,9 @@ def run_ours(args, workload):
             "gpu_launches": launches,
             "clocks": clk.summary(),
             "warp_idle_frac_last_step": st["idle_ns"] / max(1, st["warp_ns"]),
+            "phase_cycles_last_step": {k: int(st[k]) for k in ("leaf_cycles", "level_cycles", "prefix_cycles")},
+            "arenas": {"bytes": int(st["arena_bytes"]), "borrowed": int(st["borrowed_arenas"]),
+                       "pool": int(st["arena_pool"])},
         }
         if w.get("paged"):
             info = graph.info()
@@ -649,13 +678,49 @@ def run_batch_compare(args, workload):
     if args.autotune:
         from pumatch_b200 import autotune
         limit = max(10.0, 3.0 * statistics.median(batched) / 1000.0)  # a config 3x slower is not a candidate
-        rows = autotune.sweep(ctx, g, plans, warps=(4, 8, 16), chunks=(32, 256, 2048), splits=(16, 64),
+        rows = autotune.sweep(ctx, g, plans, warps=(4, 8, 16), chunks=(16, 64, 256, 2048), splits=(16, 64),
                               timeout_ms=int(limit * 1000))
         done = [r for r in rows if r["kernel_ms"] is not None]
         best = min(done, key=lambda r: r["kernel_ms"]) if done else None
         tuned = {"metric": "autotune_batched_ms", "workload": workload, "best": best,
                  "default_kernel_ms": statistics.median(batched), "configs": len(rows), "results": rows}
         print(json.dumps(tuned), flush=True)
+
+
+def run_ref_gpu_table(args):
+    """This build's kernel ms beside the reference GPU binary's, on every
+    (graph, pattern, truncation) of tests/golden/ref_gpu_counts.json (the
+    reference's own counts and kernel ms, as shipped: -G device code); the
+    counts must be the reference's."""
+    import torch
+    torch.cuda.set_device(0)
+    gold = os.path.join(ROOT, "tests", "golden")
+    recs = json.load(open(os.path.join(gold, "ref_gpu_counts.json")))
+    pats = json.load(open(os.path.join(gold, "patterns.json")))
+    ctx = pm.Context(0)
+    graphs, rows = {}, []
+    for r in recs:
+        key = (r["graph"], r["labeled"])
+        if key not in graphs:
+            hg = pm.HostGraph.read(os.path.join(gold, "graphs", r["graph"]), labeled=r["labeled"])
+            graphs[key] = pm.GraphPreprocessor.from_host(hg, labeled=r["labeled"])
+        p = pm.PatternPreprocessor(text=pats[r["pattern"]], labeled=r["labeled"])
+        times = []
+        for k in range(args.warmup + args.steps):
+            c, st = ctx.match(graphs[key], [p], truncate=r["truncate"])
+            if k >= args.warmup:
+                times.append(st["kernel_ms"])
+        rows.append({"graph": r["graph"], "pattern": r["pattern"], "labeled": r["labeled"], "truncate": r["truncate"],
+                     "count": c[0], "ref_count": r["count"], "equal": c[0] == r["count"],
+                     "ref_kernel_ms": r["ms"], "kernel_ms": statistics.median(times)})
+    for g in graphs.values():
+        g.close()
+    ctx.close()
+    line = {"metric": "reference_gpu_vs_ours_kernel_ms", "rows": rows,
+            "all_counts_equal": all(x["equal"] for x in rows),
+            "note": "reference: its own GPU binary built from its sources as shipped (-G device code), times from "
+                    "tests/golden/ref_gpu_counts.json; ours: median device time of this build's launch"}
+    print(json.dumps(line), flush=True)
 
 
 def main():
@@ -676,12 +741,18 @@ def main():
                          "(0 default, -1 never)")
     ap.add_argument("--root-limit", type=int, default=0, help="profile this many roots only (from --root-begin)")
     ap.add_argument("--root-begin", type=int, default=0)
+    ap.add_argument("--sample-roots", default="",
+                    help="sampled workloads: run only these positions of the sample (comma-separated; profiling)")
     ap.add_argument("--learned", action="store_true", help="plain vs learned scheduling on the workload")
     ap.add_argument("--learn-epochs", type=int, default=20)
     ap.add_argument("--compare-sequential", action="store_true", help="batched vs one launch per pattern")
     ap.add_argument("--autotune", action="store_true", help="with --compare-sequential: sweep launch configs")
+    ap.add_argument("--ref-gpu-table", action="store_true",
+                    help="this build's kernel ms beside the reference GPU binary's on its golden cases")
     args = ap.parse_args()
-    if args.learned:
+    if args.ref_gpu_table:
+        run_ref_gpu_table(args)
+    elif args.learned:
         run_learned(args, args.workload)
     elif args.compare_sequential:
         run_batch_compare(args, args.workload)

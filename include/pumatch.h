@@ -272,6 +272,15 @@ typedef struct {
                                order (learned binning); NULL = natural      */
   float* root_reads;        /* optional device ptr: per-root adjacency-list
                                reads (page touches when paged; plan 0)      */
+  int64_t own_arena_words;  /* candidate-set words in each warp's own arena
+                               (0 = the plans' worst case up to 65,536);
+                               warps that outgrow it borrow a worst-case
+                               arena from a pool for the rest of the root
+                               (the reference truncates instead,
+                               src/gpu_match.cu:302,316)                    */
+  int32_t max_borrowed;     /* cap on the pool of borrowed arenas (0 = as
+                               many as a quarter of free memory holds)       */
+  int32_t pad_;
 } pm_run_opts;
 
 void pm_run_opts_default(pm_run_opts* o);
@@ -298,6 +307,14 @@ typedef struct {
   uint64_t warp_ns;         /* sum over warps of their time in the launch    */
   uint64_t idle_ns;         /* sum over warps of time spent waiting for
                                donated work once the root queue was empty   */
+  uint64_t borrowed_arenas; /* times a warp borrowed a worst-case arena      */
+  uint64_t arena_pool;      /* worst-case arenas in the launch's pool        */
+  uint64_t leaf_cycles;     /* sum over warps of SM cycles counting the last
+                               level(s)                                      */
+  uint64_t level_cycles;    /* ... computing the candidate sets of the levels
+                               above it                                      */
+  uint64_t prefix_cycles;   /* ... recomputing the path prefix of a donated
+                               range (the cost of moving work between warps) */
 } pm_stats;
 
 /* Replaces the `_parallel_match` launch and the host reduction of per-warp

@@ -289,7 +289,11 @@ typedef struct {
   int64_t size[ORC_MAX_SLOTS];
   int32_t path[ORC_MAX_PAT];
   orc_stats st;
+  double deadline; /* CLOCK_MONOTONIC seconds; 0 = none (timed runs stop at it) */
+  int stopped;
 } dfs_t;
+
+static double mono_s(void);
 
 /* number of elements of a[0,len) strictly below ub (upper_bound with the
  * reference's comparison, src/gpu_match.cu:185-202) */
@@ -401,9 +405,11 @@ static uint64_t extend(dfs_t* d, int L) {
   uint64_t total = 0;
   const int64_t m = d->size[b];
   const int32_t* cand = d->buf[b];
-  for (int64_t i = 0; i < m; i++) {
+  for (int64_t i = 0; i < m && !d->stopped; i++) {
     d->path[L + 1] = cand[i];
     total += extend(d, L + 1);
+    /* timed runs: stop at the deadline, keeping the matches found so far */
+    if (d->deadline > 0 && (i & 63) == 63 && mono_s() >= d->deadline) d->stopped = 1;
   }
   return total;
 }
@@ -546,8 +552,9 @@ static void* split_worker(void* v) {
   split_arg* a = (split_arg*)v;
   dfs_t d;
   dfs_init(&d, a->g, a->p, a->T, a->maxdeg);
+  d.deadline = a->deadline;
   for (;;) {
-    if (a->deadline > 0 && mono_s() >= a->deadline) break;
+    if (d.stopped || (a->deadline > 0 && mono_s() >= a->deadline)) break;
     const int64_t i = __atomic_fetch_add(a->cursor, 1, __ATOMIC_RELAXED);
     if (i >= a->nitems) break;
     const int64_t r = a->item_root[i];
@@ -569,7 +576,7 @@ static void* split_worker(void* v) {
     }
     if (a->per_root) __atomic_fetch_add(&a->per_root[r], c, __ATOMIC_RELAXED);
     a->total += c;
-    __atomic_fetch_add(a->done, 1, __ATOMIC_RELAXED);
+    if (!d.stopped) __atomic_fetch_add(a->done, 1, __ATOMIC_RELAXED);
   }
   a->st = d.st;
   dfs_free(&d);

@@ -72,8 +72,9 @@ uint64_t orc_count_mt(const orc_graph* g, const orc_plan* p, const int32_t* root
 /* Per-root counts of roots[0, nroots) with each root's DFS divided over
  * nthreads at the candidates of level 1's main slot (the same DFS per piece,
  * so the counts are orc_count's).  Pieces run in a shuffled order when
- * shuffle_seed != 0; with time_limit_s > 0 the run stops at the limit and the
- * counts cover the pieces done (*items_done of *items_total). */
+ * shuffle_seed != 0; with time_limit_s > 0 the run stops at the limit, also
+ * inside a piece, and the counts are the matches found by then
+ * (*items_done of *items_total pieces finished). */
 uint64_t orc_count_split(const orc_graph* g, const orc_plan* p, const int32_t* roots, int64_t nroots,
                          int truncate, int nthreads, double time_limit_s, uint64_t shuffle_seed,
                          uint64_t* per_root, int64_t* items_done, int64_t* items_total, orc_stats* st);

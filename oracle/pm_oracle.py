@@ -144,9 +144,9 @@ def count_split(g: Graph, p: OrcPlan, rts: np.ndarray, threads: int = 1, time_li
                 shuffle_seed: int = 0, truncate: int = 0):
     """Raw per-root counts of the roots in `rts`, each root's DFS divided over
     `threads` at the candidates of level 1 (pieces in a seeded shuffled order
-    when shuffle_seed != 0).  With time_limit_s > 0 the run stops at the limit:
-    the counts then cover the pieces done.  Returns (total, per_root,
-    pieces_done, pieces_total, stats)."""
+    when shuffle_seed != 0).  With time_limit_s > 0 the run stops at the limit,
+    also inside a piece: the counts are then the matches found by then.
+    Returns (total, per_root, pieces_finished, pieces_total, stats)."""
     rts = np.ascontiguousarray(rts, dtype=np.int32)
     pr = np.zeros(max(len(rts), 1), dtype=np.uint64)
     done, tot = C.c_int64(), C.c_int64()

@@ -65,7 +65,8 @@ class RunOpts(C.Structure):
                 ("root_begin", C.c_int64), ("root_end", C.c_int64), ("cold_cache", C.c_int32),
                 ("high_occupancy", C.c_int32), ("leaf_per_lane", C.c_int32), ("lane_subtree_max", C.c_int32),
                 ("root_counts", C.c_void_p), ("root_cost", C.c_void_p), ("root_order", C.c_void_p),
-                ("root_reads", C.c_void_p)]
+                ("root_reads", C.c_void_p), ("own_arena_words", C.c_int64), ("max_borrowed", C.c_int32),
+                ("pad_", C.c_int32)]
 
 
 class Stats(C.Structure):
@@ -75,7 +76,9 @@ class Stats(C.Structure):
                 ("pages_loaded", C.c_uint64), ("evictions", C.c_uint64), ("kernel_ms", C.c_float),
                 ("roots_ms", C.c_float), ("grid_blocks", C.c_int32), ("block_threads", C.c_int32),
                 ("arena_bytes", C.c_uint64), ("device_status", C.c_uint32), ("pad_", C.c_uint32),
-                ("warp_ns", C.c_uint64), ("idle_ns", C.c_uint64)]
+                ("warp_ns", C.c_uint64), ("idle_ns", C.c_uint64), ("borrowed_arenas", C.c_uint64),
+                ("arena_pool", C.c_uint64), ("leaf_cycles", C.c_uint64), ("level_cycles", C.c_uint64),
+                ("prefix_cycles", C.c_uint64)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_ if not k.endswith("_")}
@@ -464,7 +467,8 @@ class Context:
         """Runs all patterns in one launch; returns (counts list, stats dict).
         Keyword arguments are pm_run_opts fields (truncate, warps_per_block,
         chunk, split_level1, shard_rank/shard_count, root_begin/root_end,
-        timeout_ms, cold_cache, high_occupancy, leaf_per_lane, lane_subtree_max, use_graph) and
+        timeout_ms, cold_cache, high_occupancy, leaf_per_lane, lane_subtree_max, use_graph,
+        own_arena_words, max_borrowed) and
         device pointers root_counts_ptr, root_cost_ptr, root_order_ptr,
         root_reads_ptr."""
         o = self._opts(**kw)

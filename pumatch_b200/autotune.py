@@ -19,24 +19,40 @@ from typing import Callable, Dict, Iterable, List, Optional, Sequence
 from . import PM_ERR_TIMEOUT, Context, GraphPreprocessor, HostGraph, PatternPreprocessor, PmError
 
 WARPS = (4, 8, 16)
-CHUNKS = (32, 64, 128, 256, 512, 1024, 2048, 4096)
+CHUNKS = (16, 32, 64, 128, 256, 512, 1024, 2048, 4096)
 SPLITS = (16, 64, 256)
+VARIANTS = (2, 3)  # kernel register caps: 85 (three 256-thread blocks per SM), uncapped
 PAGE_KB = (16, 64, 256)
+# the library's own defaults (pm_run_opts zeroed): always a candidate, so the
+# tuned configuration is never slower than the untuned one
+DEFAULT = {"warps_per_block": 8, "chunk": 16, "split_level1": 64, "high_occupancy": 0}
+
+
+def _valid(w: int, v: int) -> bool:
+    return v == 3 or w <= 8  # 16-warp blocks need the uncapped variant
 
 
 def sweep(ctx: Context, graph: GraphPreprocessor, plans: Sequence[PatternPreprocessor], *,
           warps: Iterable[int] = WARPS, chunks: Iterable[int] = CHUNKS, splits: Iterable[int] = SPLITS,
-          reps: int = 1, timeout_ms: int = 60000, extra: Optional[dict] = None) -> List[dict]:
-    """Times every (warps, chunk, split) on one placed graph."""
+          variants: Iterable[int] = VARIANTS, reps: int = 1, timeout_ms: int = 60000,
+          extra: Optional[dict] = None) -> List[dict]:
+    """Times the default configuration, then every valid (warps, chunk,
+    split, kernel variant), on one placed graph.  A configuration that hits
+    timeout_ms is dropped (kernel_ms None); one that changes a count is an
+    error."""
     extra = extra or {}
+    configs = [dict(DEFAULT, default=True)]
+    for w, c, s, v in itertools.product(warps, chunks, splits, variants):
+        if _valid(w, v):
+            configs.append({"warps_per_block": w, "chunk": c, "split_level1": s, "high_occupancy": v})
     rows = []
     want = None
-    for w, c, s in itertools.product(warps, chunks, splits):
+    for cfg in configs:
+        kw = {k: cfg[k] for k in ("warps_per_block", "chunk", "split_level1", "high_occupancy")}
         best = None
         for _ in range(reps):
             try:
-                counts, st = ctx.match(graph, list(plans), warps_per_block=w, chunk=c, split_level1=s,
-                                       timeout_ms=timeout_ms, **extra)
+                counts, st = ctx.match(graph, list(plans), timeout_ms=timeout_ms, **kw, **extra)
             except PmError as e:
                 if e.status != PM_ERR_TIMEOUT:
                     raise
@@ -44,10 +60,10 @@ def sweep(ctx: Context, graph: GraphPreprocessor, plans: Sequence[PatternPreproc
             if want is None:
                 want = counts
             if counts != want:
-                raise RuntimeError(f"config warps={w} chunk={c} split={s} changed the counts")
+                raise RuntimeError(f"config {kw} changed the counts")
             ms = st["kernel_ms"]
             best = ms if best is None else min(best, ms)
-        rows.append({"warps_per_block": w, "chunk": c, "split_level1": s, "kernel_ms": best})
+        rows.append(dict(cfg, kernel_ms=best))
     return rows
 
 

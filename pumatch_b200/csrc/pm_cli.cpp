@@ -2,7 +2,7 @@
 //
 //   test <graph-prefix> <pattern.g> [--labeled=0|1] [--truncate=N] [--device=D]
 //        [--paged] [--frame-mb=M] [--static-mb=S] [--page-kb=K] [--batch=<list file>]
-//        [--warps=W] [--chunk=C] [--split=S] [--tuned=<autotuner json>]
+//        [--warps=W] [--chunk=C] [--split=S] [--variant=V] [--tuned=<autotuner json>]
 //        [--json=<path>]
 //
 // Same positional arguments and output as the reference's driver
@@ -16,7 +16,9 @@
 // pattern in list order (ms is the shared launch time).
 // --json writes the launch's statistics (pm_stats_json) to <path>.
 // --tuned reads the "best" record the autotuner writes (warps_per_block,
-// chunk, split_level1, page_kb); explicit flags after it override it.
+// chunk, split_level1, high_occupancy, page_kb); explicit flags after it
+// override it.  --variant picks the kernel's register cap (pm_run_opts
+// high_occupancy: 1 = 64, 2 = 85, 3 = uncapped; 0 = the default).
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -55,14 +57,14 @@ int main(int argc, char** argv) {
   if (argc < 3) {
     fprintf(stderr, "usage: test <graph-prefix> <pattern.g> [--labeled=0|1] [--truncate=N] [--device=D]\n"
                     "            [--paged] [--frame-mb=M] [--static-mb=S] [--page-kb=K] [--batch=<list>]\n"
-                    "            [--warps=W] [--chunk=C] [--split=S] [--tuned=<json>] [--json=<path>]\n");
+                    "            [--warps=W] [--chunk=C] [--split=S] [--variant=V] [--tuned=<json>] [--json=<path>]\n");
     return 2;
   }
   const char* prefix = argv[1];
   std::string pattern = argv[2];
   int labeled = 1, truncate = 0, device = 0, paged = 0;
   long long frame_mb = 4096, static_mb = 0, page_kb = 64;
-  long long warps = 0, chunk = 0, split = 0;
+  long long warps = 0, chunk = 0, split = 0, variant = 0;
   std::string batch, json_path;
   for (int i = 3; i < argc; i++) {
     const char* a = argv[i];
@@ -76,11 +78,13 @@ int main(int argc, char** argv) {
       if (tuned_int(text, "chunk", &v)) chunk = v;
       if (tuned_int(text, "split_level1", &v)) split = v;
       if (tuned_int(text, "page_kb", &v)) page_kb = v;
+      if (tuned_int(text, "high_occupancy", &v)) variant = v;
     }
     else if (!strncmp(a, "--json=", 7)) json_path = a + 7;
     else if (!strncmp(a, "--warps=", 8)) warps = atoll(a + 8);
     else if (!strncmp(a, "--chunk=", 8)) chunk = atoll(a + 8);
     else if (!strncmp(a, "--split=", 8)) split = atoll(a + 8);
+    else if (!strncmp(a, "--variant=", 10)) variant = atoll(a + 10);
     else if (!strncmp(a, "--labeled=", 10)) labeled = atoi(a + 10);
     else if (!strncmp(a, "--truncate=", 11)) truncate = atoi(a + 11);
     else if (!strncmp(a, "--device=", 9)) device = atoi(a + 9);
@@ -136,6 +140,7 @@ int main(int argc, char** argv) {
   if (warps) ro.warps_per_block = (int32_t)warps;
   if (chunk) ro.chunk = (int32_t)chunk;
   if (split) ro.split_level1 = (int32_t)split;
+  if (variant) ro.high_occupancy = (int32_t)variant;
   std::vector<uint64_t> counts(plans.size(), 0);
   pm_stats st;
   s = pm_match(ctx, g, plans.data(), (int)plans.size(), &ro, counts.data(), &st);

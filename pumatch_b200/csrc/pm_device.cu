@@ -94,9 +94,19 @@ struct MatchArgs {
   unsigned long long* counts;   // [nplans]
   unsigned long long* stats;    // [16]
   unsigned int* status;
-  int32_t* arena;
+  int32_t* arena;               // the warps' own arenas
   int64_t arena_words;          // per warp, including the gather space
   int64_t slot_words;           // per warp, slots only (gather space follows)
+  int64_t gather_words;         // per warp: space for lists copied out of frames or host memory (paged)
+  // Borrowed arenas: a warp whose candidate sets or copied lists outgrow its
+  // own arena borrows one of n_big arenas sized for the plans' worst case,
+  // for the rest of the root (or donated piece) it is on.
+  int32_t* big_arena;
+  int64_t big_slot_words;       // per borrowed arena: slots
+  int64_t big_gather_words;     // per borrowed arena: gather space after the slots
+  unsigned int* big_owner;      // [n_big]: 0 free, 1 held
+  int32_t n_big;
+  int32_t pad2;
   unsigned long long* root_counts;
   float* root_cost;
   float* root_reads;
@@ -121,7 +131,8 @@ struct MatchArgs {
 };
 
 enum { ST_SETOPS = 0, ST_BYTES = 1, ST_ROOTS = 2, ST_SPLITS = 3, ST_HITS = 4, ST_MISSES = 5,
-       ST_ZC_BYTES = 6, ST_REQUESTS = 7, ST_EVICTIONS = 8, ST_DROPPED = 9, ST_WARP_NS = 10, ST_IDLE_NS = 11 };
+       ST_ZC_BYTES = 6, ST_REQUESTS = 7, ST_EVICTIONS = 8, ST_DROPPED = 9, ST_WARP_NS = 10, ST_IDLE_NS = 11,
+       ST_BORROWS = 12, ST_LEAF_CYC = 13, ST_LEVEL_CYC = 14, ST_PREFIX_CYC = 15 };
 
 #define PM_SB_MAX 512      // ints of a leaf batch's common operand kept in shared memory
 #define PM_LANE_MAX 96     // longest first operand one lane handles alone in a leaf batch
@@ -137,13 +148,19 @@ struct WarpState {
   unsigned long long next_beat;  // setops value at which to bump the heartbeat
   unsigned long long next_split; // setops value at which to look for idle warps
   unsigned long long t_start;    // %globaltimer at kernel entry (ns)
+  int32_t* arena;                // slots of the current path: the warp's own arena or a borrowed one
+  int32_t* gather;               // gather space for lists copied out of frames or host memory (paged)
+  int64_t cap;                   // slot words at `arena`
+  int32_t ghalf;                 // words in each of the two gather halves (first and second operand)
+  int32_t big;                   // borrowed arena, or -1
   int32_t pins[PM_MAX_LIST_PAGES];  // paged mode: frames pinned for a gather
   int32_t sb[PM_SB_MAX];            // leaf batches: shared copy of the common operand
 };
 
 // Per-warp work counters (registers; flushed once at kernel exit).
 struct Work {
-  unsigned long long setops, bytes, reads;
+  unsigned long long setops, bytes, reads, borrows;
+  unsigned long long leaf_cyc, level_cyc, prefix_cyc;  // SM cycles by phase (lane 0's clock)
   unsigned int err;
   PageCounters pc;
 };
@@ -222,6 +239,93 @@ __device__ __forceinline__ ListRef adj_label(const MatchArgs& a, WarpState& S, i
   return paged_list(a.pg, b + (uint64_t)r.x, r.y, gather, S.pins, w.pc);
 }
 
+// Borrows a worst-case arena for the rest of the current root: copies the
+// live slots [0, live) over (same offsets) and switches the warp to it.  The
+// warp's own arena is left as it was, so operands already resolved into it
+// stay valid.  Waits, up to the launch deadline, while every borrowed arena
+// is held; a holder never waits for another one, so holders always finish.
+// False (DEV_ARENA_OVERFLOW without a pool, DEV_TIMEOUT at the deadline) when
+// none could be had.  Kept out of line: it is rare, and it must not pull the
+// caller's counters out of registers.
+__device__ __noinline__ unsigned borrow_arena(const MatchArgs& a, WarpState& S, int64_t live) {
+  const int lane = lane_id();
+  if (S.big >= 0 || a.n_big == 0) return DEV_ARENA_OVERFLOW;
+  int got = -1;
+  if (lane == 0) {
+    const unsigned start = (unsigned)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5) % (unsigned)a.n_big;
+    while (got < 0) {
+      for (int k = 0; k < a.n_big && got < 0; k++) {
+        const int i = (int)((start + (unsigned)k) % (unsigned)a.n_big);
+        if (*(volatile unsigned int*)&a.big_owner[i] == 0u && atomicCAS(&a.big_owner[i], 0u, 1u) == 0u) got = i;
+      }
+      if (got < 0) {
+        if (global_ns() - S.t_start > a.timeout_ns) break;
+        __nanosleep(2000);
+      }
+    }
+  }
+  got = __shfl_sync(FULL, got, 0);
+  if (got < 0) return DEV_TIMEOUT;
+  int32_t* dst = a.big_arena + (int64_t)got * (a.big_slot_words + a.big_gather_words);
+  const int32_t* src = S.arena;
+  for (int64_t i = lane; i < live; i += 32) dst[i] = src[i];
+  __syncwarp();
+  if (lane == 0) {
+    S.arena = dst;
+    S.cap = a.big_slot_words;
+    S.gather = dst + a.big_slot_words;
+    S.ghalf = (int32_t)(a.big_gather_words / 2);
+    S.big = got;
+  }
+  __syncwarp();
+  return 0;
+}
+
+__device__ __forceinline__ bool borrow(const MatchArgs& a, WarpState& S, int64_t live, Work& w) {
+  const unsigned f = borrow_arena(a, S, live);
+  w.err |= f;
+  w.borrows += f ? 0 : 1;
+  return f == 0;
+}
+
+// Gives a borrowed arena back (after the warp's writes to it) and returns
+// the warp to its own arena.
+__device__ __forceinline__ void return_arena(const MatchArgs& a, WarpState& S, int32_t* own) {
+  if (S.big < 0) return;
+  __syncwarp();
+  __threadfence();
+  __syncwarp();
+  if (lane_id() == 0) {
+    atomicExch(&a.big_owner[S.big], 0u);
+    S.arena = own;
+    S.cap = a.slot_words;
+    S.gather = own + a.slot_words;
+    S.ghalf = (int32_t)(a.gather_words / 2);
+    S.big = -1;
+  }
+  __syncwarp();
+}
+
+// Room for `need` slot words from `top` on, borrowing an arena if the warp's
+// own is too small; false (w.err set) when no arena can hold them.
+__device__ __forceinline__ bool slot_room(const MatchArgs& a, WarpState& S, int64_t top, int64_t need, Work& w) {
+  if (top + need <= S.cap) return true;
+  if (!borrow(a, S, top, w)) return false;
+  if (top + need <= S.cap) return true;
+  w.err |= DEV_ARENA_OVERFLOW;
+  return false;
+}
+
+// Room for copying a list of `len` words into either gather half (slots
+// [0, live) are kept), borrowing an arena if needed.
+__device__ __forceinline__ bool gather_room(const MatchArgs& a, WarpState& S, int64_t live, int64_t len, Work& w) {
+  if (len <= S.ghalf) return true;
+  if (!borrow(a, S, live, w)) return false;
+  if (len <= S.ghalf) return true;
+  w.err |= DEV_ARENA_OVERFLOW;
+  return false;
+}
+
 // ---------------------------------------------------------------------
 // One slot of level L for the warp's current path.  Restates compute_set
 // (src/gpu_match.cu:238-319) with the operand choice of extend
@@ -229,19 +333,31 @@ __device__ __forceinline__ ListRef adj_label(const MatchArgs& a, WarpState& S, i
 // count), writes the slot to arena[top...] unless `last`.
 // ---------------------------------------------------------------------
 template <bool LABELED, bool PAGED>
-__device__ int run_slot(const MatchArgs& a, const DPlan& P, WarpState& S, int32_t* arena, int L, int s,
-                        int top, bool last, Work& w) {
+__device__ int run_slot(const MatchArgs& a, const DPlan& P, WarpState& S, int L, int s, int top, bool last,
+                        Work& w) {
   const int lane = lane_id();
   const int kind = P.kind[s];
   const int vL = S.path[L];
-  int32_t* gatherA = arena + a.slot_words;
-  int32_t* gatherB = gatherA + a.maxdeg;
   ListRef RA, RB{nullptr, 0, -1};
   // one-label masks read only that label's part of an adjacency list: same
   // survivors in the same order, no label gathers (accounting still charges
   // the whole list, as the reference scans it)
   const uint32_t mask0 = P.slot_labels[s];
   const bool by_label = LABELED && a.lab_off && __popc(mask0) == 1 && (kind != SLOT_COPY || L == 1);
+  if (PAGED) {
+    // the adjacency operands may be copied into the gather halves: make room
+    auto list_len = [&](int v) -> int64_t {
+      return by_label ? label_range(a, v, __ffs(mask0) - 1).y : (int64_t)(a.rowptr[v + 1] - a.rowptr[v]);
+    };
+    int64_t need = 0;
+    if (kind != SLOT_COPY) need = list_len(vL);
+    else if (L == 1) need = list_len(S.path[0]);
+    if (kind == SLOT_INTERSECT && L == 1) need = max(need, list_len(S.path[0]));
+    if (!gather_room(a, S, top, need, w)) return 0;
+  }
+  int32_t* arena = S.arena;
+  int32_t* gatherA = S.gather;
+  int32_t* gatherB = S.gather + S.ghalf;
   int full_len = -1;  // length of the whole list when by_label
   int full_lenB = -1; // the same for a level-1 second operand read by label (paged)
   if (by_label) {
@@ -302,11 +418,8 @@ __device__ int run_slot(const MatchArgs& a, const DPlan& P, WarpState& S, int32_
   if (fresh_unl && T && scan > T) scan = T;  // first pass keeps A's prefix
   int cnt = 0;
   // the slot holds at most the first T survivors
-  if (!last && top + ((T && scan > T) ? T : scan) > a.slot_words) {
-    w.err |= DEV_ARENA_OVERFLOW;
-    scan = 0;
-  }
-  int32_t* out = arena + top;
+  if (!last && !slot_room(a, S, top, (T && scan > T) ? T : scan, w)) scan = 0;
+  int32_t* out = S.arena + top;
   const uint32_t mask = P.slot_labels[s];
   for (int base = 0; base < scan; base += 32) {
     const int i = base + lane;
@@ -362,9 +475,15 @@ __device__ __forceinline__ int slot_bound(const DPlan& P, const WarpState& S, in
 // no scan, only the reference's accounting for the set operation it stands
 // for (its first operand's length below its bound, its result length).
 template <bool LABELED, bool PAGED>
-__device__ void alias_slot(const MatchArgs& a, const DPlan& P, WarpState& S, int32_t* arena, int L, int s, Work& w) {
+__device__ void alias_slot(const MatchArgs& a, const DPlan& P, WarpState& S, int L, int s, int live, Work& w) {
   const int t = P.alias[s];
   const int ub = slot_bound<LABELED>(P, S, L, s);
+  if (PAGED && ub != INT_MAX) {
+    const int v = P.kind[s] != SLOT_COPY ? S.path[L] : S.path[0];
+    if ((P.kind[s] != SLOT_COPY || L == 1) && !gather_room(a, S, live, (int64_t)(a.rowptr[v + 1] - a.rowptr[v]), w))
+      return;
+  }
+  const int32_t* arena = S.arena;
   int size = S.size[t];
   if (P.alias_prefix[s] && ub != INT_MAX) size = warp_lower_bound<false>(arena + S.off[t], size, ub);
   // first operand length as the reference would scan it
@@ -375,7 +494,7 @@ __device__ void alias_slot(const MatchArgs& a, const DPlan& P, WarpState& S, int
     lenA = (int)(a.rowptr[v + 1] - a.rowptr[v]);
     if (ub != INT_MAX) {
       if (PAGED) {
-        ListRef r = adj<PAGED>(a, S, v, arena + a.slot_words, w);
+        ListRef r = adj<PAGED>(a, S, v, S.gather, w);
         lenA = warp_lower_bound<PAGED>(r.p, r.len, ub, r.cg);
         __syncwarp();
         unpin(a.pg, r);
@@ -391,7 +510,7 @@ __device__ void alias_slot(const MatchArgs& a, const DPlan& P, WarpState& S, int
     lenA = (int)(a.rowptr[v + 1] - a.rowptr[v]);
     if (ub != INT_MAX) {
       if (PAGED) {
-        ListRef r = adj<PAGED>(a, S, v, arena + a.slot_words, w);
+        ListRef r = adj<PAGED>(a, S, v, S.gather, w);
         lenA = warp_lower_bound<PAGED>(r.p, r.len, ub, r.cg);
         __syncwarp();
         unpin(a.pg, r);
@@ -411,29 +530,31 @@ __device__ void alias_slot(const MatchArgs& a, const DPlan& P, WarpState& S, int
 
 // Computes every slot of level L; returns the arena top after them.
 template <bool LABELED, bool PAGED>
-__device__ __forceinline__ int run_level(const MatchArgs& a, const DPlan& P, WarpState& S, int32_t* arena,
-                                         int L, Work& w) {
+__device__ __forceinline__ int run_level(const MatchArgs& a, const DPlan& P, WarpState& S, int L, Work& w) {
   int top = S.top[L];
   for (int s = P.level_begin[L]; s < P.level_begin[L + 1]; s++) {
     if (P.alias[s] >= 0) continue;
-    const int sz = run_slot<LABELED, PAGED>(a, P, S, arena, L, s, top, false, w);
+    const int sz = run_slot<LABELED, PAGED>(a, P, S, L, s, top, false, w);
     if (lane_id() == 0) { S.off[s] = top; S.size[s] = sz; }
     top += sz;
   }
   __syncwarp();
   for (int s = P.level_begin[L]; s < P.level_begin[L + 1]; s++) {
     if (P.alias[s] < 0) continue;
-    alias_slot<LABELED, PAGED>(a, P, S, arena, L, s, w);
+    alias_slot<LABELED, PAGED>(a, P, S, L, s, top, w);
   }
   if (lane_id() == 0) S.top[L + 1] = top;
   __syncwarp();
   return top;
 }
 
-// First index of sorted A[0,len) whose element is >= x (one lane).
+// First index of sorted A[0,len) whose element is >= x (one lane).  A list
+// wholly below x (the common case for a symmetry-breaking bound) costs one
+// load instead of a dependent chain.
 template <bool CG = false>
 __device__ __forceinline__ int lane_lower_bound(const int32_t* A, int len, int x, bool cg = true) {
-  int lo = 0, hi = len;
+  if (len == 0 || ld<CG>(A + len - 1, cg) < x) return len;
+  int lo = 0, hi = len - 1;
   while (lo < hi) {
     const int mid = (lo + hi) >> 1;
     if (ld<CG>(A + mid, cg) < x) lo = mid + 1; else hi = mid;
@@ -584,8 +705,9 @@ __device__ unsigned long long leaf_flat(const MatchArgs& a, WarpState& S, const 
 //   * candidates whose first operand is longer than PM_LANE_MAX go back to the
 //     warp-cooperative run_slot.
 template <bool LABELED, bool PAGED>
-__device__ unsigned long long leaf_batch(const MatchArgs& a, const DPlan& P, WarpState& S, int32_t* arena, int L,
-                                         int b, int e, Work& w) {
+__device__ unsigned long long leaf_batch(const MatchArgs& a, const DPlan& P, WarpState& S, int L, int b, int e,
+                                         Work& w) {
+  const int32_t* arena = S.arena;
   const int lane = lane_id();
   const int s = P.last_slot;
   const int kind = P.kind[s];
@@ -676,7 +798,7 @@ __device__ unsigned long long leaf_batch(const MatchArgs& a, const DPlan& P, War
               // flight per round trip, and asks for the page
               if (ld_vol(&a.pg.page_frame[p0]) == PAGE_ABSENT) request_page(a.pg, p0, lpc);
               const int32_t* src = a.pg.host_colidx + s0;
-              int32_t* stage = arena + a.slot_words + lane * PM_LANE_MAX;
+              int32_t* stage = S.gather + lane * PM_LANE_MAX;
               for (int x = 0; x < gr.y; x += 16) {
                 int v[16];
 #pragma unroll
@@ -792,7 +914,7 @@ __device__ unsigned long long leaf_batch(const MatchArgs& a, const DPlan& P, War
       const int cc = __shfl_sync(FULL, c, src);
       if (lane == 0) S.path[Lf] = cc;
       __syncwarp();
-      cnt_warp += (unsigned long long)run_slot<LABELED, PAGED>(a, P, S, arena, Lf, s, S.top[Lf], true, w);
+      cnt_warp += (unsigned long long)run_slot<LABELED, PAGED>(a, P, S, Lf, s, S.top[Lf], true, w);
     }
   }
   if (PAGED) {
@@ -825,8 +947,9 @@ __device__ unsigned long long leaf_batch(const MatchArgs& a, const DPlan& P, War
 // operations, counts and accounting as run_level + leaf_batch; unlabeled
 // plans of the shape DPlan.l2_x describes, no truncation, X's parent at most
 // lane_subtree_max long (it is staged in shared memory).
-__device__ unsigned long long lane_subtree(const MatchArgs& a, const DPlan& P, WarpState& S, int32_t* arena,
-                                           int L, int b, int e, Work& w) {
+__device__ unsigned long long lane_subtree(const MatchArgs& a, const DPlan& P, WarpState& S, int L, int b, int e,
+                                           Work& w) {
+  int32_t* arena = S.arena;
   const int lane = lane_id();
   const int Lq = L + 1;
   const int X = P.l2_x, Y = P.l2_y, M = P.level_begin[Lq], last = P.last_slot;
@@ -964,17 +1087,25 @@ __device__ __forceinline__ void maybe_donate(const MatchArgs& a, WarpState& S, i
 // Restates match() (src/gpu_match.cu:855-1047) without deferral: every
 // branch is finished where it starts.
 template <bool LABELED, bool PAGED>
-__device__ unsigned long long dfs_from(const MatchArgs& a, const DPlan& P, WarpState& S, int32_t* arena, int L0,
-                                       int b, int e, bool counted_prefix, int plan_id, int root_id, Work& w) {
+__device__ unsigned long long dfs_from(const MatchArgs& a, const DPlan& P, WarpState& S, int L0, int b, int e,
+                                       bool counted_prefix, int plan_id, int root_id, Work& w) {
   const int lane = lane_id();
   const int n = P.nnodes;
   if (lane == 0) S.top[1] = 0;
   __syncwarp();
-  if (n == 3) return (unsigned long long)run_slot<LABELED, PAGED>(a, P, S, arena, 1, P.level_begin[1], 0, true, w);
+  if (n == 3) return (unsigned long long)run_slot<LABELED, PAGED>(a, P, S, 1, P.level_begin[1], 0, true, w);
   {
     const unsigned long long so = w.setops, by = w.bytes, rd = w.reads;
-    for (int k = 1; k <= L0 && !w.err; k++) run_level<LABELED, PAGED>(a, P, S, arena, k, w);
-    if (!counted_prefix) { w.setops = so; w.bytes = by; w.reads = rd; }
+    const long long c0 = clock64();
+    for (int k = 1; k <= L0 && !w.err; k++) run_level<LABELED, PAGED>(a, P, S, k, w);
+    if (!counted_prefix) {
+      w.setops = so;
+      w.bytes = by;
+      w.reads = rd;
+      w.prefix_cyc += (unsigned long long)(clock64() - c0);
+    } else {
+      w.level_cyc += (unsigned long long)(clock64() - c0);
+    }
   }
   if (w.err) return 0;
   unsigned long long cnt = 0;
@@ -1011,27 +1142,34 @@ __device__ unsigned long long dfs_from(const MatchArgs& a, const DPlan& P, WarpS
     if constexpr (!LABELED && !PAGED)
       subtree = P.l2_x >= 0 && L + 4 == n && it < iend && a.lane_subtree_max > 0 &&
                 S.size[P.parent[P.l2_x]] <= a.lane_subtree_max &&
-                S.top[L + 1] + 32ll * S.size[P.parent[P.l2_x]] <= a.slot_words;
+                S.top[L + 1] + 32ll * S.size[P.parent[P.l2_x]] <= S.cap;
     if (subtree) {
       const int e2 = min(iend, it + 32);
-      cnt += lane_subtree(a, P, S, arena, L, it, e2, w);
+      const long long c0 = clock64();
+      cnt += lane_subtree(a, P, S, L, it, e2, w);
+      w.leaf_cyc += (unsigned long long)(clock64() - c0);
       if (lane == 0) S.iter[L] = e2;
       __syncwarp();
     } else if (it < iend && L + 1 == n - 2) {
       const int e2 = min(iend, it + PM_LEAF_BATCH);
-      cnt += leaf_batch<LABELED, PAGED>(a, P, S, arena, L, it, e2, w);
+      const long long c0 = clock64();
+      cnt += leaf_batch<LABELED, PAGED>(a, P, S, L, it, e2, w);
+      w.leaf_cyc += (unsigned long long)(clock64() - c0);
       if (lane == 0) S.iter[L] = e2;
       __syncwarp();
       if (w.err) return 0;
     } else if (it < iend) {
-      const int v = arena[S.off[m] + it];
+      const int v = S.arena[S.off[m] + it];
       if (lane == 0) { S.iter[L] = it + 1; S.path[L + 1] = v; }
       __syncwarp();
+      const long long c0 = clock64();
       if (L + 1 == n - 2) {
-        cnt += (unsigned long long)run_slot<LABELED, PAGED>(a, P, S, arena, L + 1, P.last_slot, S.top[L + 1], true, w);
+        cnt += (unsigned long long)run_slot<LABELED, PAGED>(a, P, S, L + 1, P.last_slot, S.top[L + 1], true, w);
+        w.leaf_cyc += (unsigned long long)(clock64() - c0);
       } else {
         L++;
-        run_level<LABELED, PAGED>(a, P, S, arena, L, w);
+        run_level<LABELED, PAGED>(a, P, S, L, w);
+        w.level_cyc += (unsigned long long)(clock64() - c0);
         if (lane == 0) { S.iter[L] = 0; S.iend[L] = S.size[P.level_begin[L]]; }
         __syncwarp();
       }
@@ -1103,10 +1241,19 @@ __global__ void __launch_bounds__(MINB == 1 ? 512 : 256, MINB) match_kernel(cons
   const int lane = lane_id();
   const int wib = threadIdx.x >> 5;
   WarpState& S = smem_state[wib];
-  if (lane == 0) { S.next_beat = 0; S.next_split = 0; S.t_start = global_ns(); }
-  __syncwarp();
   const long long gw = (long long)blockIdx.x * (blockDim.x >> 5) + wib;
-  int32_t* arena = a.arena + gw * a.arena_words;
+  int32_t* own = a.arena + gw * a.arena_words;
+  if (lane == 0) {
+    S.next_beat = 0;
+    S.next_split = 0;
+    S.t_start = global_ns();
+    S.arena = own;
+    S.cap = a.slot_words;
+    S.gather = own + a.slot_words;
+    S.ghalf = (int32_t)(a.gather_words / 2);
+    S.big = -1;
+  }
+  __syncwarp();
   Work w;
   memset(&w, 0, sizeof(w));
   unsigned long long roots = 0;
@@ -1136,7 +1283,8 @@ __global__ void __launch_bounds__(MINB == 1 ? 512 : 256, MINB) match_kernel(cons
       const unsigned long long b0 = w.bytes, r0 = w.reads;
       if (lane == 0) { S.path[0] = e.x; S.path[1] = e.y; }
       __syncwarp();
-      const unsigned long long c0 = dfs_from<LABELED, PAGED>(a, P, S, arena, 1, 0, -1, true, p, (int)rid, w);
+      const unsigned long long c0 = dfs_from<LABELED, PAGED>(a, P, S, 1, 0, -1, true, p, (int)rid, w);
+      return_arena(a, S, own);
       local += c0;
       roots++;
       if (lane == 0 && p == 0) {
@@ -1168,8 +1316,9 @@ __global__ void __launch_bounds__(MINB == 1 ? 512 : 256, MINB) match_kernel(cons
       }
       __syncwarp();
       const unsigned long long b0 = w.bytes, r0 = w.reads;
-      const unsigned long long c0 = dfs_from<LABELED, PAGED>(a, P, S, arena, item.level, item.begin, item.end,
-                                                             false, item.plan, item.root, w);
+      const unsigned long long c0 = dfs_from<LABELED, PAGED>(a, P, S, item.level, item.begin, item.end, false,
+                                                             item.plan, item.root, w);
+      return_arena(a, S, own);
       if (lane == 0) {
         if (c0) atomicAdd(&a.counts[item.plan], c0);
         if (item.plan == 0) {
@@ -1187,9 +1336,10 @@ __global__ void __launch_bounds__(MINB == 1 ? 512 : 256, MINB) match_kernel(cons
     }
     unsigned int act = 0;
     unsigned long long head = 0, tail = 0, beat = 0;
+    // no fence between these reads: a stale pair can only make a warp leave
+    // early, and the warp holding the work finishes (and drains) it itself
     if (lane == 0) {
       act = *((volatile unsigned int*)a.active);
-      __threadfence();
       head = *((volatile unsigned long long*)a.don_head);
       tail = *((volatile unsigned long long*)a.don_tail);
       beat = *((volatile unsigned long long*)a.heartbeat);
@@ -1216,6 +1366,10 @@ __global__ void __launch_bounds__(MINB == 1 ? 512 : 256, MINB) match_kernel(cons
     atomicAdd(&a.stats[ST_SETOPS], w.setops);
     atomicAdd(&a.stats[ST_BYTES], w.bytes + 8ull * roots);
     atomicAdd(&a.stats[ST_ROOTS], roots);
+    if (w.borrows) atomicAdd(&a.stats[ST_BORROWS], w.borrows);
+    atomicAdd(&a.stats[ST_LEAF_CYC], w.leaf_cyc);
+    atomicAdd(&a.stats[ST_LEVEL_CYC], w.level_cyc);
+    atomicAdd(&a.stats[ST_PREFIX_CYC], w.prefix_cyc);
     if (PAGED) {
       atomicAdd(&a.stats[ST_HITS], w.pc.hits);
       atomicAdd(&a.stats[ST_MISSES], w.pc.misses);
@@ -1815,6 +1969,8 @@ extern "C" pm_status pm_debug_roots(pm_ctx* c, const pm_graph* g, const pm_plan*
 // One prepared persistent launch: plans, roots, geometry, kernel arguments.
 struct Launch {
   bool labeled = false, paged = false, cold = false;
+  int64_t n_big = 0;          // borrowed arenas
+  size_t own_bytes = 0, big_bytes = 0;
   int nplans = 0;
   const Plan* plans[PM_MAX_BATCH];
   DPlan dp[PM_MAX_BATCH];
@@ -1828,6 +1984,10 @@ struct Launch {
 };
 
 static constexpr unsigned kDonSlots = 1u << 15;
+// a warp's own arena: at most this many slot words and gather words
+static constexpr int64_t kOwnSlotWords = 1 << 16;
+static constexpr int64_t kOwnGatherWords = 1 << 15;
+static constexpr size_t kBigPoolMaxBytes = 48ull << 30;
 static constexpr int kCtlRead = 32 + 32 + 16 + 1;  // cursors, counts, stats, status word
 
 // Validates the plans and options, builds the root lists into *roots,
@@ -1881,10 +2041,20 @@ static pm_status setup_launch(pm_ctx* c, const pm_graph* g, const pm_plan* const
     off += (size_t)L->dp[i].nroots;
     L->dp[i].nroots = e - b;
   }
-  const int64_t slot_words = arena_words;
-  // gather space for multi-page lists (two operands), at least a short list
-  // per lane for the last level's copies of lists on missing pages
-  if (L->paged) arena_words += std::max<int64_t>(2 * (int64_t)g->maxdeg + 64, 32 * PM_LANE_MAX);
+  // Candidate storage.  worst_* hold every materialised slot at its largest
+  // possible size (and, paged, two gathered max-degree lists); each warp's own
+  // arena holds that when it is small, else a bounded part of it, and warps
+  // that outgrow theirs borrow one of a pool of worst-case arenas.
+  const int64_t worst_slots = arena_words;
+  const int64_t worst_gather =
+      L->paged ? ((std::max<int64_t>(2 * (int64_t)g->maxdeg + 64, 32 * PM_LANE_MAX) + 1) & ~1ll) : 0;
+  const int64_t own_slots = std::min<int64_t>(worst_slots, o.own_arena_words > 0 ? o.own_arena_words : kOwnSlotWords);
+  const int64_t own_gather =
+      L->paged ? ((std::max<int64_t>(std::min<int64_t>(worst_gather, kOwnGatherWords), 32 * PM_LANE_MAX) + 1) & ~1ll)
+               : 0;
+  const bool borrowing = own_slots < worst_slots || own_gather < worst_gather;
+  const int64_t slot_words = own_slots;
+  arena_words = own_slots + own_gather;
 
   // launch geometry: persistent, occupancy-limited
   L->threads = wpb * 32;
@@ -1920,8 +2090,24 @@ static pm_status setup_launch(pm_ctx* c, const pm_graph* g, const pm_plan* const
     L->blocks -= c->nsm;
     L->warps = (int64_t)L->blocks * wpb;
   }
-  pm_status st = ensure((void**)arena, arena_bytes, (size_t)(L->warps * arena_words * 4));
+  // borrowed arenas: as many as a quarter of the free memory holds (capped),
+  // at least one, at most one per warp
+  const int64_t big_words = borrowing ? worst_slots + worst_gather : 0;
+  int64_t n_big = 0;
+  if (borrowing) {
+    const size_t own_b = (size_t)(L->warps * arena_words * 4);
+    const size_t room = free_b / 2 > own_b ? free_b / 2 - own_b : 0;
+    const size_t budget = std::min(room / 2, kBigPoolMaxBytes);
+    n_big = std::max<int64_t>(1, std::min<int64_t>(L->warps, (int64_t)(budget / ((size_t)big_words * 4))));
+    if (o.max_borrowed > 0) n_big = std::min<int64_t>(n_big, o.max_borrowed);
+  }
+  const size_t own_bytes = (size_t)(L->warps * arena_words * 4);
+  const size_t big_bytes = (size_t)n_big * (size_t)big_words * 4;
+  pm_status st = ensure((void**)arena, arena_bytes, own_bytes + big_bytes + 4 * (size_t)n_big + 256);
   if (st != PM_OK) return st;
+  L->n_big = n_big;
+  L->own_bytes = own_bytes;
+  L->big_bytes = big_bytes;
   // control block: cursors[32] counts[32] stats[16] status/active head tail
   // heartbeat, donation ready[] and items[]
   L->ctl_words = 32 + 32 + 16 + 8 + kDonSlots + 6 * kDonSlots;
@@ -1963,6 +2149,12 @@ static pm_status setup_launch(pm_ctx* c, const pm_graph* g, const pm_plan* const
   a.arena = *arena;
   a.arena_words = arena_words;
   a.slot_words = slot_words;
+  a.gather_words = arena_words - slot_words;
+  a.n_big = (int32_t)n_big;
+  a.big_arena = n_big ? (int32_t*)((char*)*arena + own_bytes) : nullptr;
+  a.big_slot_words = worst_slots;
+  a.big_gather_words = worst_gather;
+  a.big_owner = n_big ? (unsigned int*)((char*)*arena + own_bytes + big_bytes) : nullptr;
   a.root_counts = (unsigned long long*)o.root_counts;
   a.root_cost = o.root_cost;
   a.root_reads = o.root_reads;
@@ -1984,6 +2176,7 @@ static pm_status setup_launch(pm_ctx* c, const pm_graph* g, const pm_plan* const
 static pm_status enqueue_launch(pm_ctx* c, Launch& L, const unsigned int* active_src,
                                 unsigned long long* host_ctl, cudaEvent_t eb, cudaEvent_t ee) {
   CK(cudaMemsetAsync(L.a.cursors, 0, L.ctl_words * 8, c->stream));
+  if (L.n_big) CK(cudaMemsetAsync(L.a.big_owner, 0, 4 * (size_t)L.n_big, c->stream));
   CK(cudaMemcpyAsync(L.a.active, active_src, sizeof(unsigned int), cudaMemcpyHostToDevice, c->stream));
   if (eb) CK(cudaEventRecord(eb, c->stream));
   PM_CK_PENDING("pm_match");
@@ -2021,7 +2214,12 @@ static pm_status finish_launch(const Launch& L, const unsigned long long* host_c
     so.roots_ms = roots_ms;
     so.grid_blocks = L.blocks;
     so.block_threads = L.threads;
-    so.arena_bytes = (uint64_t)(L.warps * L.a.arena_words * 4);
+    so.arena_bytes = (uint64_t)(L.own_bytes + L.big_bytes);
+    so.borrowed_arenas = stt[ST_BORROWS];
+    so.leaf_cycles = stt[ST_LEAF_CYC];
+    so.level_cycles = stt[ST_LEVEL_CYC];
+    so.prefix_cycles = stt[ST_PREFIX_CYC];
+    so.arena_pool = (uint64_t)L.n_big;
     so.device_status = status;
   }
   if (status & DEV_ARENA_OVERFLOW) return fail(PM_ERR_INTERNAL, "device: candidate set exceeded the warp arena");
@@ -2354,6 +2552,8 @@ extern "C" pm_status pm_match_static(const uint64_t* d_rowptr, const int32_t* d_
   a.arena = arena;
   a.arena_words = slot_words;
   a.slot_words = slot_words;
+  a.gather_words = 0;
+  a.n_big = 0;
   a.timeout_ns = (unsigned long long)(o.timeout_ms > 0 ? o.timeout_ms : 600000) * 1000000ull;
   const unsigned int active0 = (unsigned int)warps;
   CK(cudaMemcpyAsync(a.active, &active0, sizeof(active0), cudaMemcpyHostToDevice, st));
@@ -2366,6 +2566,7 @@ extern "C" pm_status pm_match_static(const uint64_t* d_rowptr, const int32_t* d_
   Launch L;
   L.nplans = 1;
   L.plans[0] = &p;
+  L.own_bytes = (size_t)warps * (size_t)slot_words * 4;
   L.blocks = (int)blocks;
   L.threads = wpb * 32;
   L.warps = warps;

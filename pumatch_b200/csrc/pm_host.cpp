@@ -366,7 +366,8 @@ extern "C" pm_status pm_stats_json(const pm_stats* st, const uint64_t* counts, i
            "\"set_ops\": %llu, \"alg_bytes\": %llu, \"alg_gbs\": %.6g, \"splits\": %llu, "
            "\"page_hits\": %llu, \"page_misses\": %llu, \"pages_loaded\": %llu, \"h2d_page_bytes\": %llu, "
            "\"zero_copy_bytes\": %llu, \"evictions\": %llu, \"warp_idle_share\": %.4f, "
-           "\"grid_blocks\": %d, \"block_threads\": %d, \"device_status\": %u}",
+           "\"grid_blocks\": %d, \"block_threads\": %d, \"arena_bytes\": %llu, \"borrowed_arenas\": %llu, "
+           "\"arena_pool\": %llu, \"device_status\": %u}",
            st->kernel_ms, st->roots_ms, s > 0 ? (double)total / s : 0.0, (unsigned long long)st->n_roots,
            (unsigned long long)st->set_ops, (unsigned long long)st->alg_bytes,
            s > 0 ? (double)st->alg_bytes / s / 1e9 : 0.0, (unsigned long long)st->splits,
@@ -374,7 +375,8 @@ extern "C" pm_status pm_stats_json(const pm_stats* st, const uint64_t* counts, i
            (unsigned long long)st->pages_loaded, (unsigned long long)st->h2d_page_bytes,
            (unsigned long long)st->zero_copy_bytes, (unsigned long long)st->evictions,
            st->warp_ns ? (double)st->idle_ns / (double)st->warp_ns : 0.0, st->grid_blocks, st->block_threads,
-           st->device_status);
+           (unsigned long long)st->arena_bytes, (unsigned long long)st->borrowed_arenas,
+           (unsigned long long)st->arena_pool, st->device_status);
   j += tmp;
   if (len_out) *len_out = j.size() + 1;
   if (j.size() + 1 > cap) return fail(PM_ERR_INVALID, "pm_stats_json: needs %zu bytes", j.size() + 1);

@@ -63,21 +63,43 @@ def run_resumable(run_range: Callable[[int, int], Sequence[int]], n_roots: int, 
     return [int(x) for x in state["counts"]]
 
 
-def job_key(graph_info: dict, plan_descs: Sequence[dict], options: dict) -> str:
-    """A digest naming a job: the placed graph's shape, the compiled plans and
-    the run options that change counts."""
-    blob = json.dumps({"graph": graph_info, "plans": list(plan_descs), "options": options}, sort_keys=True,
-                      default=str)
+def job_key(graph_info: dict, plan_descs: Sequence[dict], options: dict, content: Sequence[str] = ()) -> str:
+    """A digest naming a job: the placed graph's shape, the compiled plans,
+    the run options that change counts, and digests of what the shape does
+    not pin (each plan's root list -- the graph's edges and labels as the
+    query sees them -- and a root order)."""
+    blob = json.dumps({"graph": graph_info, "plans": list(plan_descs), "options": options,
+                       "content": list(content)}, sort_keys=True, default=str)
     return hashlib.sha256(blob.encode()).hexdigest()
 
 
-def match_resumable(ctx, graph, plans, state_path: str, chunk_roots: int = 65536, **run_kw) -> List[int]:
+def roots_digest(ctx, graph, plan) -> str:
+    """sha256 of a plan's root list on a placed graph (reference order)."""
+    return hashlib.sha256(ctx.roots(graph, plan).tobytes()).hexdigest()
+
+
+def match_resumable(ctx, graph, plans, state_path: str, chunk_roots: int = 65536, root_order=None,
+                    **run_kw) -> List[int]:
     """Context.match over all root edges, one launch per range of chunk_roots
     root positions, resumable from state_path.  Counts equal one full
-    launch's."""
+    launch's.  root_order (single plan): a host int32 array of root ids, the
+    order positions are taken in; it is part of the job's key."""
+    if "root_order_ptr" in run_kw or "root_begin" in run_kw or "root_end" in run_kw:
+        raise ValueError("pass root_order as a host array; root ranges are this function's to choose")
     n_roots = max(ctx.count_roots(graph, p) for p in plans)
     info = {k: v for k, v in graph.info().items() if k in ("n_vertices", "n_adj", "max_degree", "labeled", "n_labels")}
-    key = job_key(info, [p.describe() for p in plans], {"truncate": run_kw.get("truncate", 0)})
+    content = [roots_digest(ctx, graph, p) for p in plans]
+    order_dev = None
+    if root_order is not None:
+        import numpy as np
+        import torch
+        order = np.ascontiguousarray(root_order, dtype=np.int32)
+        if len(plans) != 1 or len(order) != n_roots:
+            raise ValueError("root_order needs one plan and one entry per root")
+        content.append("order:" + hashlib.sha256(order.tobytes()).hexdigest())
+        order_dev = torch.from_numpy(order).to(f"cuda:{ctx.device}")
+        run_kw["root_order_ptr"] = order_dev.data_ptr()
+    key = job_key(info, [p.describe() for p in plans], {"truncate": run_kw.get("truncate", 0)}, content)
 
     def run_range(b, e):
         counts, _ = ctx.match(graph, list(plans), root_begin=b, root_end=e, **run_kw)

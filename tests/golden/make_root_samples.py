@@ -15,9 +15,10 @@ count (x |Aut| when unlabeled) and the set operations, which the GPU's
 per-root counts and launch statistics must equal.
 
 The graph is built by the oracle's generator (the workload definition the
-product's generator implements; a CPU test pins the two equal), and its
-arrays' sha256 is stored so a run on another machine can check it has the
-same graph.
+product's generator implements; a CPU test pins the two equal) -- or, for a
+graph too large to sort on a host, by the product's device generator, which a
+GPU test pins to the host generator -- and its arrays' sha256 is stored so a
+run on another machine can check it has the same graph.
 """
 from __future__ import annotations
 
@@ -44,13 +45,30 @@ SAMPLES = {
     "chunglu100k_c7": dict(graph=dict(kind="chung_lu", n=100_000, m=1_000_000, gamma=2.1, i0=10.0, max_w=5000.0,
                                       seed=1),
                            labeled=False, pattern=P.to_g(*P.cycle(7)), perm_seed=7, budget=5e9,
-                           est_probes=400, est_seed=11),
+                           budget_kind="set_ops", est_probes=400, est_seed=11, max_looked=20000,
+                           query_probes=20000),
+    # the configured R-MAT query: 65M vertices, 1.8e9 undirected edges (a, b, c
+    # = .57, .19, .19, seed 2), 8 uniform labels (seed 102), the 5-cycle plus a
+    # 2-vertex pendant path with labels drawn from the 8 (seed 202).  Its
+    # graph is built on a GPU (the device generator returns the host
+    # generator's arrays) in a machine with ~100 GB of free RAM; the budget is
+    # in algorithmic bytes, the oracle's cost on hub lists.
+    "rmat65m_c5t2_lab8": dict(graph=dict(kind="rmat", n=65_000_000, m=1_800_000_000, a=0.57, b=0.19, c=0.19,
+                                         seed=2, device=0),
+                              labeled=True, n_labels=8, label_seed=102,
+                              pattern=P.to_g(*P.cycle_tail(5, 2), P.seeded_labels(7, 8, 202)), perm_seed=7,
+                              budget=2e12, budget_kind="alg_bytes", est_probes=100, est_seed=11, max_looked=3000,
+                              query_probes=2000),
 }
 
 
 def build_graph(gd):
     if gd["kind"] == "chung_lu":
         return orc.gen_chung_lu(gd["n"], gd["m"], gd["gamma"], gd["i0"], gd["max_w"], gd["seed"])
+    if "device" in gd:  # too large for a host sort: the product's device generator (same arrays)
+        import pumatch_b200 as pm
+        hg = pm.gen_rmat(gd["n"], gd["m"], a=gd["a"], b=gd["b"], c=gd["c"], seed=gd["seed"], device=gd["device"])
+        return hg.rowptr, hg.colidx
     return orc.gen_rmat(gd["n"], gd["m"], gd["a"], gd["b"], gd["c"], gd["seed"])
 
 
@@ -64,13 +82,17 @@ def graph_digest(rowptr: np.ndarray, colidx: np.ndarray) -> str:
 def choose(g, p, roots, spec):
     perm = np.random.default_rng(spec["perm_seed"]).permutation(len(roots))
     kept, total, looked = [], 0.0, 0
+    by_bytes = spec.get("budget_kind") == "alg_bytes"
     for i in perm:
         looked += 1
-        so, _, _ = orc.estimate(g, p, roots[i:i + 1], probes=spec["est_probes"], seed=spec["est_seed"])
-        if so > spec["budget"]:
+        so, by, _ = orc.estimate(g, p, roots[i:i + 1], probes=spec["est_probes"], seed=spec["est_seed"])
+        cost = by if by_bytes else so
+        if looked > spec["max_looked"]:
+            break
+        if cost > spec["budget"]:
             continue
         kept.append((int(i), so))
-        total += so
+        total += cost
         if total >= spec["budget"]:
             break
     return kept, looked
@@ -79,7 +101,8 @@ def choose(g, p, roots, spec):
 def make(name, threads):
     spec = SAMPLES[name]
     rp, ci = build_graph(spec["graph"])
-    g = orc.Graph(rp, ci, None)
+    labels = orc.gen_labels(len(rp) - 1, spec["n_labels"], spec["label_seed"]) if spec["labeled"] else None
+    g = orc.Graph(rp, ci, labels)
     p = orc.plan(spec["pattern"], spec["labeled"])
     roots = orc.roots(g, p)
     kept, looked = choose(g, p, roots, spec)
@@ -88,13 +111,15 @@ def make(name, threads):
     total, per_root, done, pieces, st = orc.count_split(g, p, roots[idx], threads=threads)
     assert done == pieces
     mult = 1 if spec["labeled"] else p.multiplicity
-    so_total, _, _ = orc.estimate(g, p, roots, probes=20000, seed=spec["est_seed"])
+    so_total, _, _ = orc.estimate(g, p, roots, probes=spec["query_probes"], seed=spec["est_seed"])
     rec = {
         "graph": spec["graph"], "graph_sha256": graph_digest(rp, ci), "n_adj": int(len(ci)),
         "labeled": spec["labeled"], "pattern": spec["pattern"], "multiplicity": int(mult),
         "rule": (f"seeded permutation (numpy default_rng({spec['perm_seed']})) of the {len(roots)} root edges; "
                  f"keep roots whose Knuth estimate ({spec['est_probes']} probes, seed {spec['est_seed']}) is at "
-                 f"most {spec['budget']:.0e} set operations until the kept estimates sum to {spec['budget']:.0e}"),
+                 f"most {spec['budget']:.0e} {spec.get('budget_kind', 'set_ops').replace('_', ' ')} until the "
+                 f"kept estimates sum to {spec['budget']:.0e}"),
+        "n_labels": spec.get("n_labels", 0), "label_seed": spec.get("label_seed"),
         "n_roots_total": int(len(roots)), "roots_examined": looked,
         "query_set_ops_estimate": so_total,
         "roots": [{"index": int(i), "v0": int(roots[i][0]), "v1": int(roots[i][1]), "raw_count": int(c),
@@ -120,7 +145,8 @@ def main():
         if args.only and name != args.only:
             continue
         out[name] = make(name, args.threads)
-        print(name, out[name]["count"], out[name]["set_ops"], out[name]["oracle_s"], "s", flush=True)
+        print(name, len(out[name]["roots"]), "roots", out[name]["count"], out[name]["set_ops"],
+              out[name]["oracle_s"], "s", flush=True)
         with open(args.out, "w") as f:
             json.dump(out, f, indent=1)
 

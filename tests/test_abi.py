@@ -146,9 +146,12 @@ def test_new_fields_match_c():
 #include <stddef.h>
 #include "pumatch.h"
 int main(void){
- printf("%zu %zu %zu %zu %zu %zu\n", offsetof(pm_graph_opts, static_pool_bytes), offsetof(pm_graph_info, n_static_frames),
+ printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\n", offsetof(pm_graph_opts, static_pool_bytes),
+        offsetof(pm_graph_info, n_static_frames),
         offsetof(pm_run_opts, leaf_per_lane), offsetof(pm_run_opts, lane_subtree_max), offsetof(pm_stats, warp_ns),
-        offsetof(pm_stats, idle_ns));
+        offsetof(pm_stats, idle_ns), offsetof(pm_run_opts, own_arena_words), offsetof(pm_run_opts, max_borrowed),
+        offsetof(pm_stats, borrowed_arenas), offsetof(pm_stats, arena_pool), sizeof(pm_run_opts), sizeof(pm_stats));
+ printf("%zu %zu %zu\n", offsetof(pm_stats, leaf_cycles), offsetof(pm_stats, level_cycles), offsetof(pm_stats, prefix_cycles));
  return 0; }'''
     import ctypes as C
     import tempfile
@@ -159,7 +162,10 @@ int main(void){
     vals = [int(x) for x in subprocess.run([os.path.join(d, "p")], capture_output=True, text=True).stdout.split()]
     assert vals == [pm.GraphOpts.static_pool_bytes.offset, pm.GraphInfo.n_static_frames.offset,
                     pm.RunOpts.leaf_per_lane.offset, pm.RunOpts.lane_subtree_max.offset, pm.Stats.warp_ns.offset,
-                    pm.Stats.idle_ns.offset]
+                    pm.Stats.idle_ns.offset, pm.RunOpts.own_arena_words.offset, pm.RunOpts.max_borrowed.offset,
+                    pm.Stats.borrowed_arenas.offset, pm.Stats.arena_pool.offset, C.sizeof(pm.RunOpts),
+                    C.sizeof(pm.Stats), pm.Stats.leaf_cycles.offset, pm.Stats.level_cycles.offset,
+                    pm.Stats.prefix_cycles.offset]
 
 
 def test_c_program_links_and_runs_host_entry_points(tmp_path):
@@ -203,6 +209,7 @@ def test_stats_json_sidecar():
     st = pm.Stats()
     st.kernel_ms, st.n_roots, st.set_ops, st.alg_bytes = 2000.0, 7, 11, 4_000_000_000
     st.page_hits, st.warp_ns, st.idle_ns, st.grid_blocks = 5, 1000, 250, 444
+    st.borrowed_arenas, st.arena_pool = 3, 9
     counts = (C.c_uint64 * 2)(10, 2**63)
     need = C.c_size_t()
     assert pm.lib().pm_stats_json(C.byref(st), counts, 2, None, 0, C.byref(need)) == pm.PM_ERR_INVALID
@@ -213,3 +220,4 @@ def test_stats_json_sidecar():
     assert abs(d["alg_gbs"] - 2.0) < 1e-9 and abs(d["warp_idle_share"] - 0.25) < 1e-9
     assert abs(d["matches_per_s"] - (10 + 2**63) / 2.0) / d["matches_per_s"] < 1e-6
     assert d["grid_blocks"] == 444 and d["device_status"] == 0
+    assert d["borrowed_arenas"] == 3 and d["arena_pool"] == 9

@@ -263,8 +263,8 @@ def test_gpu_cli_output(tmp_path):
     assert int(r.stdout.strip().splitlines()[-1].split()[1]) == want
     # launch configuration from an autotuner record, then overridden by a flag
     tuned = tmp_path / "tuned.json"
-    tuned.write_text('{"best": {"warps_per_block": 4, "chunk": 32, "split_level1": 16, "page_kb": null, '
-                     '"kernel_ms": 1.0}, "results": []}')
+    tuned.write_text('{"best": {"warps_per_block": 16, "chunk": 32, "split_level1": 16, "high_occupancy": 3, '
+                     '"page_kb": null, "kernel_ms": 1.0}, "results": []}')
     r = subprocess.run([pm.CLI_PATH, prefix, str(pat), "--tuned=" + str(tuned), "--chunk=8"], capture_output=True,
                        text=True, cwd=tmp_path)
     assert r.returncode == 0, r.stderr

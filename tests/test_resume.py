@@ -78,6 +78,29 @@ def test_job_key_changes_with_what_changes_counts():
     assert a == resume.job_key({"n_vertices": 5}, [{"nslots": 3}], {"truncate": 0})
     assert a != resume.job_key({"n_vertices": 6}, [{"nslots": 3}], {"truncate": 0})
     assert a != resume.job_key({"n_vertices": 5}, [{"nslots": 3}], {"truncate": 16})
+    # same shape, other edges (root lists differ) or another root order: another job
+    assert a != resume.job_key({"n_vertices": 5}, [{"nslots": 3}], {"truncate": 0}, ["roots-x"])
+    assert (resume.job_key({"n_vertices": 5}, [{"nslots": 3}], {"truncate": 0}, ["roots-x"])
+            != resume.job_key({"n_vertices": 5}, [{"nslots": 3}], {"truncate": 0}, ["roots-x", "order:1"]))
+
+
+def test_same_shape_other_edges_gives_another_key():
+    """Two graphs of one shape (vertices, adjacency entries, max degree) but
+    different edges: their root lists differ, so their jobs do."""
+    import hashlib
+
+    import numpy as np
+    rp = np.array([0, 2, 4, 6, 8], dtype=np.uint64)
+    a = np.array([1, 2, 0, 3, 0, 3, 1, 2], dtype=np.int32)  # 4-cycle 0-1-3-2-0
+    b = np.array([1, 3, 0, 2, 1, 3, 0, 2], dtype=np.int32)  # 4-cycle 0-1-2-3-0
+    p = orc.plan(P.to_g(*P.path(3)), False)
+    keys = []
+    for ci in (a, b):
+        g = orc.Graph(rp, ci, None)
+        digest = hashlib.sha256(np.ascontiguousarray(orc.roots(g, p), dtype=np.int32).tobytes()).hexdigest()
+        keys.append(resume.job_key({"n_vertices": 4, "n_adj": 8, "max_degree": 2}, [{"p": 1}], {"truncate": 0},
+                                   [digest]))
+    assert keys[0] != keys[1]
 
 
 @pytest.mark.gpu
@@ -92,6 +115,15 @@ def test_gpu_match_resumable_equals_one_launch(tmp_path):
         path = str(tmp_path / "state.json")
         assert resume.match_resumable(ctx, g, plans, path, chunk_roots=997) == want
         assert resume.match_resumable(ctx, g, plans, path, chunk_roots=997) == want  # finished state
+        # a root order is part of the job: its state file is another job's
+        import numpy as np
+        n = ctx.count_roots(g, plans[0])
+        order = np.random.default_rng(3).permutation(n).astype(np.int32)
+        want1, _ = ctx.match(g, plans[:1])
+        with pytest.raises(ValueError):
+            resume.match_resumable(ctx, g, plans[:1], path, chunk_roots=997, root_order=order)
+        p2 = str(tmp_path / "state2.json")
+        assert resume.match_resumable(ctx, g, plans[:1], p2, chunk_roots=997, root_order=order) == want1
         g.close()
     finally:
         ctx.close()
