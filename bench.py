@@ -144,13 +144,13 @@ def build_workload(name, graph_seed=None, via_oracle=False):
     return w, hg, texts
 
 
-def load_sample(w, hg):
+def load_sample(w, hg, path=None):
     """The workload's root sample record, after checking that this graph is
     the one the sample was drawn on (arrays' sha256)."""
     if "sample" not in w:
         return None
     import hashlib
-    with open(SAMPLES_PATH) as f:
+    with open(path or SAMPLES_PATH) as f:
         rec = json.load(f)[w["sample"]]
     h = hashlib.sha256()
     h.update(hg.rowptr.tobytes())
@@ -164,10 +164,17 @@ def sample_config(rec):
     if rec is None:
         return None
     k = len(rec["roots"])
-    return {"rule": rec["rule"], "roots": k, "of": rec["n_roots_total"],
-            "root_ids": [r["index"] for r in rec["roots"]], "set_ops": rec["set_ops"],
-            "query_set_ops_estimate": rec["query_set_ops_estimate"],
-            "share_of_query": rec["set_ops"] / rec["query_set_ops_estimate"]}
+    extra = rec.get("extra_roots") or []
+    out = {"rule": rec["rule"], "roots": k + len(extra), "of": rec["n_roots_total"],
+           "root_ids": [r["index"] for r in rec["roots"]] + [r["index"] for r in extra],
+           "oracle_verified_roots": k, "verified_set_ops": rec["set_ops"],
+           "query_set_ops_estimate": rec["query_set_ops_estimate"]}
+    if extra:
+        out["extra_rule"] = rec.get("extra_rule")
+        out["extra_set_ops_estimate"] = sum(r["set_ops_estimate"] for r in extra)
+    else:
+        out["share_of_query"] = rec["set_ops"] / rec["query_set_ops_estimate"]
+    return out
 
 
 def place_graph(w, hg, device):
@@ -281,7 +288,8 @@ def cpu_measure(hg, texts, labeled, threads, sample=None, time_limit_s=15.0, see
     mult = [1 if labeled else p.multiplicity for p in plans]
     if sample is not None:
         p = plans[0]
-        rts = orc.roots(g, p)[[r["index"] for r in sample["roots"]]]
+        ids = [r["index"] for r in sample["roots"]] + [r["index"] for r in (sample.get("extra_roots") or [])]
+        rts = orc.roots(g, p)[ids]
         t0 = time.perf_counter()
         c, _, done, tot, _ = orc.count_split(g, p, rts, threads=threads, time_limit_s=time_limit_s,
                                              shuffle_seed=seed)
@@ -325,7 +333,7 @@ def run_reference(args, workload):
     if rank != 0:
         return
     w, hg, texts = build_workload(workload, via_oracle=True)
-    sample = load_sample(w, hg)
+    sample = load_sample(w, hg, args.samples)
     threads = os.cpu_count() or 1
     for k in range(args.warmup):
         cpu_measure(hg, texts, w["labeled"], threads, sample, time_limit_s=2.0, seed=99 + k)
@@ -362,12 +370,12 @@ def run_ours(args, workload):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local))
     w, hg, texts = build_workload(workload)
-    sample = load_sample(w, hg)
-    subset = False
+    sample = load_sample(w, hg, args.samples)
+    subset = bool(sample and sample.get("extra_roots"))
     if sample is not None and args.sample_roots:
         # profiling a part of the sample: its roots' counts are still checked
         keep = [int(x) for x in args.sample_roots.split(",")]
-        sample = dict(sample, roots=[sample["roots"][i] for i in keep])
+        sample = dict(sample, roots=[sample["roots"][i] for i in keep], extra_roots=[])
         sample["raw_count"] = sum(r["raw_count"] for r in sample["roots"])
         sample["count"] = sum(r["count"] for r in sample["roots"])
         subset = True
@@ -393,10 +401,12 @@ def run_ours(args, workload):
         roots_all = ctx.roots(graph, plans[0])
         if len(roots_all) != sample["n_roots_total"]:
             raise SystemExit("root list length differs from the sample's")
-        for r in sample["roots"]:
+        for r in sample["roots"] + (sample.get("extra_roots") or []):
             if tuple(roots_all[r["index"]]) != (r["v0"], r["v1"]):
                 raise SystemExit(f"root {r['index']} is not the sampled edge")
-        order_h = torch.tensor([r["index"] for r in sample["roots"]], dtype=torch.int32).pin_memory()
+        del roots_all
+        ids = [r["index"] for r in sample["roots"]] + [r["index"] for r in (sample.get("extra_roots") or [])]
+        order_h = torch.tensor(ids, dtype=torch.int32).pin_memory()
         order = order_h.to("cuda")
         run_kw.update(root_order_ptr=order.data_ptr(), root_begin=0, root_end=len(order_h))
 
@@ -496,11 +506,13 @@ def run_ours(args, workload):
         if sample is not None:
             # every sampled root against the oracle's exact per-root count
             bad = [r["index"] for r in sample["roots"] if int(per_root_gpu[r["index"]]) != r["raw_count"]]
-            ok = (not bad and counts_total[0] == sample["count"] and
-                  (subset or (set_ops // args.steps == sample["set_ops"] and
+            verified = sum(int(per_root_gpu[r["index"]]) for r in sample["roots"]) * mult
+            ok = (not bad and verified == sample["count"] and
+                  (subset or (counts_total[0] == sample["count"] and set_ops // args.steps == sample["set_ops"] and
                               alg_bytes // args.steps == sample["alg_bytes"])))
             parity = {"roots_checked": len(sample["roots"]), "ok": ok, "mismatched_roots": bad,
-                      "count": counts_total[0], "oracle_count": sample["count"],
+                      "roots_not_checked": len(sample.get("extra_roots") or []),
+                      "count_checked_roots": verified, "oracle_count": sample["count"],
                       "set_ops_equal": None if subset else set_ops // args.steps == sample["set_ops"],
                       "alg_bytes_equal": None if subset else alg_bytes // args.steps == sample["alg_bytes"],
                       "against": "oracle exact per-root counts, set operations and algorithmic bytes "
@@ -514,7 +526,7 @@ def run_ours(args, workload):
                        "patterns": [p for p, _ in texts], "counts": counts_total,
                        "root_sample": sample_config(sample),
                        "kernel_variant": ["default", "regs64", "regs85", "uncapped"][args.high_occupancy] +
-                                         ("+leaf_per_lane" if args.leaf_per_lane else "") +
+                                         ({0: "", 1: "+leaf_per_lane", 2: "+leaf_strided"}[args.leaf_per_lane]) +
                                          (f"+lane_subtree_max={args.lane_subtree_max}"
                                           if args.lane_subtree_max else ""),
                        "root_limit": args.root_limit or None,
@@ -734,13 +746,15 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--high-occupancy", type=int, default=0,
                     help="kernel variant: 0 default, 1 capped at 64 registers, 2 capped at 85, 3 uncapped")
-    ap.add_argument("--leaf-per-lane", action="store_true",
-                    help="last level one candidate per lane instead of work-balanced across the warp")
+    ap.add_argument("--leaf-per-lane", type=int, default=0,
+                    help="last level: 0 work-balanced in lane-contiguous parts (default), 1 one candidate per "
+                         "lane, 2 work-balanced strided")
     ap.add_argument("--lane-subtree-max", type=int, default=0,
                     help="clique-like plans: last two levels one candidate per lane up to this parent size "
                          "(0 default, -1 never)")
     ap.add_argument("--root-limit", type=int, default=0, help="profile this many roots only (from --root-begin)")
     ap.add_argument("--root-begin", type=int, default=0)
+    ap.add_argument("--samples", default=None, help="root-sample fixture file (default tests/golden/root_samples.json)")
     ap.add_argument("--sample-roots", default="",
                     help="sampled workloads: run only these positions of the sample (comma-separated; profiling)")
     ap.add_argument("--learned", action="store_true", help="plain vs learned scheduling on the workload")

@@ -260,7 +260,10 @@ typedef struct {
   int32_t leaf_per_lane;    /* 1: last-level intersections one candidate per
                                lane (long lists go to the warp); 0 (default):
                                work-balanced across the warp when the common
-                               operand fits in shared memory                 */
+                               operand fits in shared memory, each lane
+                               walking a contiguous part of the candidates'
+                               lists; 2: the same, strided (lane l takes
+                               every 32nd element)                           */
   int32_t lane_subtree_max; /* unlabeled plans ending in a chain of
                                intersections (cliques): the last two levels
                                run one candidate per lane when the parent set

@@ -78,7 +78,8 @@ struct MatchArgs {
   const int32_t* colidx_lab;    // label-grouped lists (labeled, HBM) or null
   const int32_t* lab_off;       // label group offsets (labeled, HBM or paged) or null
   const int32_t* host_sorted;   // labeled paged: the id-sorted lists in mapped host memory
-  int32_t leaf_flat;            // last-level intersections work-balanced across the warp (leaf_flat)
+  int32_t leaf_flat;            // last level: 0 one candidate per lane, 1 flat in lane-contiguous parts,
+                                // 2 flat strided (leaf_flat)
   int32_t lane_subtree_max;     // lane_subtree when the parent set is at most this long; 0 = never
   int32_t nl1;
   int32_t pad1;
@@ -137,6 +138,7 @@ enum { ST_SETOPS = 0, ST_BYTES = 1, ST_ROOTS = 2, ST_SPLITS = 3, ST_HITS = 4, ST
 #define PM_SB_MAX 512      // ints of a leaf batch's common operand kept in shared memory
 #define PM_LANE_MAX 96     // longest first operand one lane handles alone in a leaf batch
 #define PM_LEAF_BATCH 512  // candidates per leaf batch
+#define PM_WIN 256         // window of a merged second operand held in shared memory
 
 struct WarpState {
   int32_t path[8];
@@ -154,7 +156,10 @@ struct WarpState {
   int32_t ghalf;                 // words in each of the two gather halves (first and second operand)
   int32_t big;                   // borrowed arena, or -1
   int32_t pins[PM_MAX_LIST_PAGES];  // paged mode: frames pinned for a gather
-  int32_t sb[PM_SB_MAX];            // leaf batches: shared copy of the common operand
+  int32_t sb[PM_SB_MAX];            // leaf batches: the common operand (bitmap, hash table or sorted copy)
+  int32_t wb[PM_WIN];               // intersections by merge: the current window of the second operand
+  unsigned long long lrb[32];       // leaf batches: start of each candidate's first operand in colidx
+  int32_t lexcl[33];                // leaf batches: offset of each candidate's operand in the flat layout
 };
 
 // Per-warp work counters (registers; flushed once at kernel exit).
@@ -421,12 +426,40 @@ __device__ int run_slot(const MatchArgs& a, const DPlan& P, WarpState& S, int L,
   if (!last && !slot_room(a, S, top, (T && scan > T) ? T : scan, w)) scan = 0;
   int32_t* out = S.arena + top;
   const uint32_t mask = P.slot_labels[s];
+  // an intersection whose second operand is not in shared memory and not
+  // much longer than the scanned part of the first: merge, B streamed through
+  // shared memory in coalesced windows; else a search per element of A
+  const bool merge = kind == SLOT_INTERSECT && B != S.sb && lenB > PM_WIN && (long long)lenB <= 32ll * scan;
+  int bpos = 0;  // merge: B[0, bpos) is below every element still to come
   for (int base = 0; base < scan; base += 32) {
     const int i = base + lane;
     const bool valid = i < scan;
     const int x = valid ? ld<PAGED>(A + i, cgA) : 0;
     bool keep = valid;
-    if (kind == SLOT_INTERSECT && keep) keep = bsearch_in<PAGED>(B, lenB, x, cgB);
+    if (merge) {
+      const int xlo = __shfl_sync(FULL, x, 0);
+      const int xhi = __shfl_sync(FULL, x, min(31, scan - 1 - base));
+      bpos += warp_lower_bound<PAGED>(B + bpos, lenB - bpos, xlo, cgB);
+      bool open = valid;  // this lane's membership still undecided
+      keep = false;
+      while (__any_sync(FULL, open)) {
+        const int wn = min(PM_WIN, lenB - bpos);
+        if (wn <= 0) break;  // B exhausted: the rest of the tile is not in B
+        __syncwarp();
+        for (int k = lane; k < wn; k += 32) S.wb[k] = ld<PAGED>(B + bpos + k, cgB);
+        __syncwarp();
+        const int wlast = S.wb[wn - 1];
+        if (open && x <= wlast) {
+          keep = bsearch_in<false>(S.wb, wn, x);
+          open = false;
+        }
+        if (xhi <= wlast) break;
+        bpos += wn;
+      }
+      // bpos stays at the last window: it may hold elements of the next tile
+    } else if (kind == SLOT_INTERSECT && keep) {
+      keep = bsearch_in<PAGED>(B, lenB, x, cgB);
+    }
     if (LABELED) {
       if (keep && !by_label) keep = (mask >> a.labels[x]) & 1u;
     } else if (kind == SLOT_COPY) {
@@ -614,35 +647,136 @@ __device__ __forceinline__ bool in_table(const int32_t* t, int bits, int x) {
   }
 }
 
+// Membership structures for a leaf batch's common operand B (sorted), built
+// in the warp's shared staging buffer (PM_SB_MAX words):
+enum : int {
+  MEMB_BITMAP = 0,  // max B < 32 * PM_SB_MAX: one bit per id in [0, max B]
+  MEMB_FILTER = 1,  // |B| <= PM_SB_MAX / 4: a one-hash filter of 16 * PM_SB_MAX bits, then a hash table
+  MEMB_HASH = 2,    // |B| <= PM_SB_MAX / 2: an open-addressing table at most half full
+  MEMB_SORTED = 3   // else: the sorted copy, binary search
+};
+
+struct LeafSet {
+  const int32_t* t;
+  int bits;       // hash table: log2(slots)
+  int lo, hi;     // min and max of B: outside [lo, hi] nothing is a member
+};
+
+__device__ __forceinline__ unsigned leaf_hash(int x, int bits) { return ((unsigned)x * 0x9E3779B1u) >> (32 - bits); }
+
+template <int MODE>
+__device__ __forceinline__ bool leaf_member(const LeafSet& m, int lenB, int x) {
+  if (x < m.lo || x > m.hi) return false;
+  if (MODE == MEMB_BITMAP) return (((const unsigned int*)m.t)[x >> 5] >> (x & 31)) & 1u;
+  if (MODE == MEMB_FILTER) {
+    const unsigned f = ((unsigned)x * 0x2545F491u) >> 19;  // 13 bits: PM_SB_MAX / 2 words of filter
+    if (!((((const unsigned int*)m.t)[f >> 5] >> (f & 31)) & 1u)) return false;
+    return in_table(m.t + PM_SB_MAX / 2, m.bits, x);
+  }
+  if (MODE == MEMB_HASH) return in_table(m.t, m.bits, x);
+  return bsearch_in<false>(m.t, lenB, x);
+}
+
+// Builds the structure for B (whole warp) and returns its mode.
+__device__ int leaf_build(WarpState& S, const int32_t* B, int lenB, LeafSet& m) {
+  const int lane = lane_id();
+  m.t = S.sb;
+  m.lo = lenB ? B[0] : 1;
+  m.hi = lenB ? B[lenB - 1] : 0;
+  m.bits = 5;
+  int mode;
+  if (m.hi < 32 * PM_SB_MAX) {
+    mode = MEMB_BITMAP;
+    const int words = lenB ? (m.hi >> 5) + 1 : 0;
+    for (int i = lane; i < words; i += 32) S.sb[i] = 0;
+    __syncwarp();
+    for (int i = lane; i < lenB; i += 32) atomicOr((unsigned int*)&S.sb[B[i] >> 5], 1u << (B[i] & 31));
+  } else if (lenB <= PM_SB_MAX / 2) {
+    mode = lenB <= PM_SB_MAX / 4 ? MEMB_FILTER : MEMB_HASH;
+    int32_t* tab = S.sb + (mode == MEMB_FILTER ? PM_SB_MAX / 2 : 0);
+    const int cap = mode == MEMB_FILTER ? PM_SB_MAX / 2 : PM_SB_MAX;
+    while ((1 << m.bits) < 2 * lenB) m.bits++;
+    if (mode == MEMB_FILTER) {
+      while ((2 << m.bits) <= cap && (1 << m.bits) < 4 * lenB) m.bits++;  // at most a quarter full
+      for (int i = lane; i < PM_SB_MAX / 2; i += 32) S.sb[i] = 0;
+    }
+    const int size = 1 << m.bits;  // <= cap
+    for (int i = lane; i < size; i += 32) tab[i] = -1;
+    __syncwarp();
+    for (int i = lane; i < lenB; i += 32) {
+      const int x = B[i];
+      if (mode == MEMB_FILTER) {
+        const unsigned f = ((unsigned)x * 0x2545F491u) >> 19;
+        atomicOr((unsigned int*)&S.sb[f >> 5], 1u << (f & 31));
+      }
+      unsigned h = leaf_hash(x, m.bits);
+      while (atomicCAS(&tab[h], -1, x) != -1) h = (h + 1) & (unsigned)(size - 1);
+    }
+  } else {
+    mode = MEMB_SORTED;
+    for (int i = lane; i < lenB; i += 32) S.sb[i] = B[i];
+  }
+  __syncwarp();
+  return mode;
+}
+
+// One lane's contiguous part [t, tend) of a leaf batch's flat layout
+// (candidate j's first operand occupies [lexcl[j], lexcl[j+1]) and starts at
+// colidx[lrb[j]]): members of B, label-checked when LABELED.
+template <bool LABELED, int MODE>
+__device__ __forceinline__ unsigned leaf_walk(const MatchArgs& a, const WarpState& S, const LeafSet& m, int lenB,
+                                              uint32_t mask, int t, int tend) {
+  unsigned k = 0;
+  int j = 0;  // the last candidate whose offset is <= t
+#pragma unroll
+  for (int step = 16; step; step >>= 1)
+    if (S.lexcl[j + step] <= t) j += step;
+  while (t < tend) {
+    const int jbeg = S.lexcl[j];
+    const int stop = min(tend, S.lexcl[j + 1]);
+    const int32_t* src = a.colidx + S.lrb[j] + (unsigned long long)(t - jbeg);
+    const int n = stop - t;
+    int q = 0;
+    for (; q + 4 <= n; q += 4) {
+      int x[4];
+#pragma unroll
+      for (int u = 0; u < 4; u++) x[u] = src[q + u];
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+        bool hit = leaf_member<MODE>(m, lenB, x[u]);
+        if (LABELED && hit) hit = (mask >> a.labels[x[u]]) & 1u;
+        k += hit ? 1u : 0u;
+      }
+    }
+    for (; q < n; q++) {
+      const int x = src[q];
+      bool hit = leaf_member<MODE>(m, lenB, x);
+      if (LABELED && hit) hit = (mask >> a.labels[x]) & 1u;
+      k += hit ? 1u : 0u;
+    }
+    t = stop;
+    j++;
+  }
+  return k;
+}
+
 // The last-level intersections of candidates [b, e) with the common operand B
 // (|B| <= PM_SB_MAX), work-balanced across the warp: the first operands of 32
 // candidates (each cut at its symmetry-breaking bound) are laid end to end
-// and every lane takes every 32nd element, finds its owner by a binary
-// search over the lanes' offsets, and tests it against B in shared memory
-// (a hash table when |B| <= PM_SB_MAX / 2, else the sorted copy).  Counts
-// only; no truncation.  Same set operations, counts and accounting as
-// lane_intersect per candidate.
+// and split into 32 contiguous parts, one per lane.  A lane finds the
+// candidate owning its part's start once and walks on through the following
+// lists, four loads in flight, testing each element against B's structure in
+// shared memory (leaf_build).  Counts only; no truncation.  Same set
+// operations, counts and accounting as lane_intersect per candidate.
+// a.leaf_flat == 2 selects the earlier strided layout (element t0 + lane,
+// owner found per element by shuffles), kept for comparison.
 template <bool LABELED>
 __device__ unsigned long long leaf_flat(const MatchArgs& a, WarpState& S, const int32_t* cand, int b, int e,
                                         const int32_t* B, int lenB, uint32_t mask, int common_ub, bool self_ub,
                                         Work& w) {
   const int lane = lane_id();
-  const bool hashed = lenB <= PM_SB_MAX / 2;
-  int bits = 5;
-  if (hashed) {
-    while ((1 << bits) < 2 * lenB) bits++;  // 2^bits <= PM_SB_MAX
-    const int size = 1 << bits;
-    for (int i = lane; i < size; i += 32) S.sb[i] = -1;
-    __syncwarp();
-    for (int i = lane; i < lenB; i += 32) {
-      const int x = B[i];
-      unsigned h = ((unsigned)x * 0x9E3779B1u) >> (32 - bits);
-      while (atomicCAS(&S.sb[h], -1, x) != -1) h = (h + 1) & (unsigned)(size - 1);
-    }
-  } else {
-    for (int i = lane; i < lenB; i += 32) S.sb[i] = B[i];
-  }
-  __syncwarp();
+  LeafSet m;
+  const int mode = leaf_build(S, B, lenB, m);
   unsigned long long cnt = 0, bytes = 0, ops = 0;  // per lane
   for (int base = b; base < e; base += 32) {
     const int i = base + lane;
@@ -663,24 +797,44 @@ __device__ unsigned long long leaf_flat(const MatchArgs& a, WarpState& S, const 
       const int t = __shfl_up_sync(FULL, incl, o);
       if (lane >= o) incl += t;
     }
-    const int excl = incl - lenA;
     const int total = __shfl_sync(FULL, incl, 31);
-    for (int t0 = 0; t0 < total; t0 += 32) {
-      const int t = t0 + lane;
-      int j = 0, ej = 0;  // the last lane whose offset is <= t owns element t
+    if (a.leaf_flat == 2) {
+      const int excl = incl - lenA;
+      for (int t0 = 0; t0 < total; t0 += 32) {
+        const int t = t0 + lane;
+        int j = 0, ej = 0;  // the last lane whose offset is <= t owns element t
 #pragma unroll
-      for (int step = 16; step; step >>= 1) {
-        const int e2 = __shfl_sync(FULL, excl, j + step);
-        if (e2 <= t) { j += step; ej = e2; }
+        for (int step = 16; step; step >>= 1) {
+          const int e2 = __shfl_sync(FULL, excl, j + step);
+          if (e2 <= t) { j += step; ej = e2; }
+        }
+        const unsigned long long rbj = __shfl_sync(FULL, rb, j);
+        if (t < total) {
+          const int x = a.colidx[rbj + (unsigned long long)(t - ej)];
+          bool hit = mode == MEMB_BITMAP   ? leaf_member<MEMB_BITMAP>(m, lenB, x)
+                     : mode == MEMB_FILTER ? leaf_member<MEMB_FILTER>(m, lenB, x)
+                     : mode == MEMB_HASH   ? leaf_member<MEMB_HASH>(m, lenB, x)
+                                           : leaf_member<MEMB_SORTED>(m, lenB, x);
+          if (LABELED && hit) hit = (mask >> a.labels[x]) & 1u;
+          cnt += hit ? 1u : 0u;
+        }
       }
-      const unsigned long long rbj = __shfl_sync(FULL, rb, j);
-      if (t < total) {
-        const int x = a.colidx[rbj + (unsigned long long)(t - ej)];
-        bool hit = hashed ? in_table(S.sb, bits, x) : bsearch_in<false>(S.sb, lenB, x);
-        if (LABELED && hit) hit = (mask >> a.labels[x]) & 1u;
-        cnt += hit ? 1u : 0u;
-      }
+      continue;
     }
+    S.lrb[lane] = rb;
+    S.lexcl[lane] = incl - lenA;
+    if (lane == 31) S.lexcl[32] = total;
+    __syncwarp();
+    const int chunk = (total + 31) >> 5;
+    const int t = min(total, lane * chunk);
+    const int tend = min(total, t + chunk);
+    unsigned k;
+    if (mode == MEMB_BITMAP) k = leaf_walk<LABELED, MEMB_BITMAP>(a, S, m, lenB, mask, t, tend);
+    else if (mode == MEMB_FILTER) k = leaf_walk<LABELED, MEMB_FILTER>(a, S, m, lenB, mask, t, tend);
+    else if (mode == MEMB_HASH) k = leaf_walk<LABELED, MEMB_HASH>(a, S, m, lenB, mask, t, tend);
+    else k = leaf_walk<LABELED, MEMB_SORTED>(a, S, m, lenB, mask, t, tend);
+    cnt += k;
+    __syncwarp();
   }
   bytes += 4ull * cnt;  // the results
   for (int o = 16; o; o >>= 1) {
@@ -2122,7 +2276,7 @@ static pm_status setup_launch(pm_ctx* c, const pm_graph* g, const pm_plan* const
   a.colidx_lab = g->d_colidx_lab;
   a.lab_off = g->d_lab_off;
   a.host_sorted = (g->residency == PM_RESIDENT_PAGED && g->d_lab_off) ? g->h_colidx_dev : nullptr;
-  a.leaf_flat = o.leaf_per_lane ? 0 : 1;
+  a.leaf_flat = o.leaf_per_lane == 1 ? 0 : (o.leaf_per_lane == 2 ? 2 : 1);
   a.lane_subtree_max = lane_subtree_limit(o);
   a.nl1 = g->nl1;
   a.n = (int32_t)g->n;
@@ -2525,7 +2679,7 @@ extern "C" pm_status pm_match_static(const uint64_t* d_rowptr, const int32_t* d_
   a.rowptr = d_rowptr;
   a.colidx = d_colidx;
   a.labels = d_labels;
-  a.leaf_flat = o.leaf_per_lane ? 0 : 1;
+  a.leaf_flat = o.leaf_per_lane == 1 ? 0 : (o.leaf_per_lane == 2 ? 2 : 1);
   a.lane_subtree_max = lane_subtree_limit(o);
   a.n = (int32_t)n;
   a.nplans = 1;

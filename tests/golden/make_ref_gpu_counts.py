@@ -10,7 +10,10 @@ this repository.
     python tests/golden/make_ref_gpu_counts.py --out ref_gpu_counts.json
 
 Each record: graph, pattern, labeled, truncate (the binary's GRAPH_DEGREE),
-count (last stdout line of the binary), ms.  Unlabeled patterns whose last
+count (last stdout line of the binary), ms.  The committed fixture is the
+union of two runs (--graphs cl400,dense60, then --graphs rmat512,cl3000);
+cases whose binary crashed twice on the host (SIGSEGV in the reference's
+helper threads, no GPU fault) are absent.  Unlabeled patterns whose last
 vertex is a fresh neighbour set are skipped: there the reference diffs a slot
 it never wrote (src/gpu_match.cu:292 vs 534-568), so its count depends on
 stale device memory.
