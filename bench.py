@@ -92,9 +92,20 @@ WORKLOADS = {
                                     paged=dict(frame_bytes=4 << 30, static_bytes=0, page_bytes=64 << 10)),
     "rmat65m_c5t2_lab8": dict(graph=_RMAT65M, labeled=True, n_labels=8, label_seed=102, pattern_label_seed=202,
                               patterns=[("C5t2", P.cycle_tail(5, 2))], sample="rmat65m_c5t2_lab8"),
+    # the configured batch: twenty seeded 4-7-vertex patterns (8 labels) on the
+    # configured R-MAT graph, paged through the 4 GB pool, over a slice of
+    # each pattern's root list (--root-frac, --root-limit)
+    "rmat65m_batch20_lab8_paged": dict(graph=_RMAT65M, labeled=True, n_labels=8, label_seed=102, batch_seed=303,
+                                       paged=dict(frame_bytes=4 << 30, static_bytes=0, page_bytes=64 << 10)),
     # twenty seeded 4-7-vertex patterns in one persistent launch
     "rmat128k_batch20_lab32": dict(graph=_RMAT128K, labeled=True, n_labels=32, label_seed=102, batch_seed=303),
-    # learned-scheduler comparison (--learned): trained on seeds 11, 12, 13
+    # learned-scheduler comparison (--learned): trained on seeds 11, 12, 13;
+    # a frame pool of a quarter of the adjacency, all of it under CLOCK
+    "rmat128k_c5t2_lab32_clock": dict(graph=_RMAT128K, labeled=True, n_labels=32, label_seed=102,
+                                      pattern_label_seed=202, patterns=[("C5t2", P.cycle_tail(5, 2))],
+                                      paged=dict(frame_fraction=0.25, static_fraction=0.0, page_bytes=16 << 10)),
+    # the same graph with the reference's split: 60% of the adjacency in
+    # static frames plus 28% evictable
     "rmat128k_c5t2_lab32_paged": dict(graph=_RMAT128K, labeled=True, n_labels=32, label_seed=102,
                                       pattern_label_seed=202, patterns=[("C5t2", P.cycle_tail(5, 2))],
                                       paged=dict(frame_fraction=0.88, static_fraction=0.6, page_bytes=16 << 10)),
@@ -583,17 +594,22 @@ def run_ours(args, workload):
 
 
 def run_learned(args, workload):
-    """Plain vs learned (heavy-first root order + learned page residency) on
-    the workload's graph, the model trained on plain runs over three other
-    seeds of the same generator.  Counts must be identical."""
+    """Plain vs learned on the workload's paged graph, the model trained on
+    plain runs over three other seeds of the same generator.
+
+    plain: the frame pool starts cold (only static frames) and pages in on
+    demand under CLOCK, roots in reference order.  learned: the pool starts
+    with the pages the model predicts hottest, roots heaviest-first, and each
+    root chunk's predicted pages are posted to the copy ring a few chunks
+    ahead during the run.  Counts must be identical."""
     import torch
 
     from pumatch_b200 import learn
     torch.cuda.set_device(0)
     ctx = pm.Context(0)
     w, hg, texts = build_workload(workload)
-    if len(texts) != 1:
-        raise SystemExit("--learned needs a single-pattern workload")
+    if len(texts) != 1 or not w.get("paged"):
+        raise SystemExit("--learned needs a single-pattern paged workload")
     labeled = w["labeled"]
     xs, ts = [], []
     t0 = time.time()
@@ -613,25 +629,35 @@ def run_learned(args, workload):
     g = place_graph(w, hg, 0)
     xe = learn.root_features(ctx, g, p)
     pred = model.predict(xe)
-    count, st, cost, reads = learn.plain_costs(ctx, g, p, timeout_ms=args.timeout_s * 1000)
+    # the evaluation graph's own per-root costs, from a plain run, judge the prediction
+    hb = pm.GraphPreprocessor.from_host(hg, labeled=labeled)
+    count, st0, cost, reads = learn.plain_costs(ctx, hb, p, timeout_ms=args.timeout_s * 1000)
+    hb.close()
     te = learn.targets(cost, reads)
     mae = (pred - te).abs().mean(0).tolist()
     base = (te - t.mean(0)).abs().mean(0).tolist()
     order = learn.heavy_first_order(pred)
-    if w.get("paged"):
-        info = g.info()
-        roots = ctx.roots(g, p)
-        score = learn.page_scores(hg.rowptr, roots, torch.expm1(pred[:, 1].clamp_min(0)).cpu().numpy(),
-                                  w["paged"]["page_bytes"] // 4, info["n_pages"])
-    kw = dict(timeout_ms=args.timeout_s * 1000)
+    info = g.info()
+    roots = ctx.roots(g, p)
+    pred_reads = torch.expm1(pred[:, 1].clamp_min(0)).cpu().numpy()
+    page_ints = w["paged"]["page_bytes"] // 4
+    score = learn.page_scores(hg.rowptr, roots, pred_reads, page_ints, info["n_pages"])
+    chunk = 16
+    pf_off, pf_pages = learn.prefetch_lists(hg.rowptr, hg.colidx, roots, order.cpu().numpy(), pred_reads, page_ints,
+                                            chunk, per_chunk=args.prefetch_pages)
+    pf_off_d = torch.from_numpy(pf_off).cuda()
+    pf_pages_d = torch.from_numpy(pf_pages if len(pf_pages) else np.zeros(1, dtype=np.int32)).cuda()
+    kw = dict(timeout_ms=args.timeout_s * 1000, chunk=chunk)
+    arms = {
+        "plain": dict(cold_cache=1),
+        "learned_residency_order": dict(root_order_ptr=order.data_ptr()),
+        "learned": dict(root_order_ptr=order.data_ptr(), prefetch_off_ptr=pf_off_d.data_ptr(),
+                        prefetch_pages_ptr=pf_pages_d.data_ptr(), prefetch_chunks=len(pf_off) - 1),
+    }
+    hot = np.argsort(-score)[:info["n_frames"] - info["n_static_frames"]]
     res = {}
-    for mode in ("plain", "learned"):
-        if w.get("paged"):
-            # plain: the first pages of the array (the reference's device
-            # partition); learned: the pages the model predicts hottest
-            pages = np.arange(info["n_frames"]) if mode == "plain" else np.argsort(-score)[:info["n_frames"]]
-            g.set_resident_pages(pages)
-        extra = dict(root_order_ptr=order.data_ptr()) if mode == "learned" else {}
+    for mode, extra in arms.items():
+        g.set_resident_pages(hot if mode != "plain" else np.zeros(0, dtype=np.int64))
         times, stats = [], None
         for k in range(args.warmup + args.steps):
             c, stt = ctx.match(g, [p], **kw, **extra)
@@ -639,20 +665,26 @@ def run_learned(args, workload):
             if k >= args.warmup:
                 times.append(stt["kernel_ms"])
                 stats = stt
-        res[mode] = {"kernel_ms": statistics.median(times), "page_misses": stats["page_misses"],
-                     "pages_loaded": stats["pages_loaded"], "zero_copy_bytes": stats["zero_copy_bytes"],
-                     "splits": stats["splits"]}
+        res[mode] = {"kernel_ms": statistics.median(times), "page_hits": stats["page_hits"],
+                     "page_misses": stats["page_misses"], "pages_loaded": stats["pages_loaded"],
+                     "zero_copy_bytes": stats["zero_copy_bytes"], "h2d_page_bytes": stats["h2d_page_bytes"],
+                     "prefetch_requests": stats["prefetch_requests"], "splits": stats["splits"]}
     line = {"metric": "query_ms_learned_vs_plain", "workload": workload, "count": count,
-            "plain": res["plain"], "learned": res["learned"],
-            "speedup": res["plain"]["kernel_ms"] / res["learned"]["kernel_ms"],
+            "arms": res, "speedup": res["plain"]["kernel_ms"] / res["learned"]["kernel_ms"],
+            "plain": "cold frame pool, CLOCK, reference root order",
+            "learned": "predicted-hot pages resident, heaviest-first roots, predicted pages prefetched per chunk",
             "prediction_mae_log": mae, "constant_predictor_mae_log": base, "train_loss": [hist[0], hist[-1]],
-            "train_s": train_s, "train_roots": int(x.shape[0]), "eval_roots": int(xe.shape[0])}
+            "train_s": train_s, "train_roots": int(x.shape[0]), "eval_roots": int(xe.shape[0]),
+            "frames": int(info["n_frames"]), "pages": int(info["n_pages"]),
+            "prefetch_pages_listed": int(len(pf_pages))}
     print(json.dumps(line), flush=True)
 
 
 def run_batch_compare(args, workload):
     """One batched persistent launch (and its CUDA-graph replay) vs the same
-    patterns launched one by one; optional autotuner sweep."""
+    patterns launched one by one, over the same roots; optional autotuner
+    sweep.  With --root-frac/--root-limit every pattern runs the root
+    positions [f * L, f * L + limit) of its list, L the shortest list."""
     import torch
     torch.cuda.set_device(0)
     ctx = pm.Context(0)
@@ -661,6 +693,12 @@ def run_batch_compare(args, workload):
     g = place_graph(w, hg, 0)
     plans = [pm.PatternPreprocessor(text=t, labeled=labeled) for _, t in texts]
     kw = dict(timeout_ms=args.timeout_s * 1000)
+    rng = None
+    if args.root_limit > 0:
+        shortest = min(ctx.count_roots(g, p) for p in plans)
+        b = int(args.root_frac * shortest)
+        rng = (b, b + args.root_limit)
+        kw.update(root_begin=rng[0], root_end=rng[1])
     for _ in range(args.warmup):
         ctx.match(g, plans, **kw)
     batched = []
@@ -673,6 +711,7 @@ def run_batch_compare(args, workload):
         cq, sq = q.run()
         assert cq == c
         replay.append(sq["kernel_ms"])
+    q.close()
     seq = []
     for _ in range(args.steps):
         tot, cs = 0.0, []
@@ -683,20 +722,26 @@ def run_batch_compare(args, workload):
         assert cs == c
         seq.append(tot)
     line = {"metric": "batched_vs_sequential_ms", "workload": workload, "patterns": [n for n, _ in texts],
-            "counts": c, "batched_ms": statistics.median(batched), "graph_replay_kernel_ms": statistics.median(replay),
-            "sequential_ms": statistics.median(seq),
-            "speedup": statistics.median(seq) / statistics.median(batched)}
+            "counts": c, "root_range": rng, "batched_ms": statistics.median(batched),
+            "graph_replay_kernel_ms": statistics.median(replay), "sequential_ms": statistics.median(seq),
+            "speedup": statistics.median(seq) / statistics.median(batched),
+            "counts_equal": "batched, graph replay and sequential"}
+    if w.get("paged"):
+        line["paged"] = w["paged"]
     print(json.dumps(line), flush=True)
     if args.autotune:
         from pumatch_b200 import autotune
         limit = max(10.0, 3.0 * statistics.median(batched) / 1000.0)  # a config 3x slower is not a candidate
+        extra = {k: v for k, v in kw.items() if k != "timeout_ms"}
         rows = autotune.sweep(ctx, g, plans, warps=(4, 8, 16), chunks=(16, 64, 256, 2048), splits=(16, 64),
-                              timeout_ms=int(limit * 1000))
+                              timeout_ms=int(limit * 1000), extra=extra)
         done = [r for r in rows if r["kernel_ms"] is not None]
         best = min(done, key=lambda r: r["kernel_ms"]) if done else None
         tuned = {"metric": "autotune_batched_ms", "workload": workload, "best": best,
-                 "default_kernel_ms": statistics.median(batched), "configs": len(rows), "results": rows}
+                 "default": rows[0], "configs": len(rows), "results": rows}
         print(json.dumps(tuned), flush=True)
+    g.close()
+    ctx.close()
 
 
 def run_ref_gpu_table(args):
@@ -754,11 +799,14 @@ def main():
                          "(0 default, -1 never)")
     ap.add_argument("--root-limit", type=int, default=0, help="profile this many roots only (from --root-begin)")
     ap.add_argument("--root-begin", type=int, default=0)
+    ap.add_argument("--root-frac", type=float, default=0.0,
+                    help="with --compare-sequential: start the root slice at this fraction of the shortest list")
     ap.add_argument("--samples", default=None, help="root-sample fixture file (default tests/golden/root_samples.json)")
     ap.add_argument("--sample-roots", default="",
                     help="sampled workloads: run only these positions of the sample (comma-separated; profiling)")
     ap.add_argument("--learned", action="store_true", help="plain vs learned scheduling on the workload")
     ap.add_argument("--learn-epochs", type=int, default=20)
+    ap.add_argument("--prefetch-pages", type=int, default=64, help="learned: pages listed per root chunk")
     ap.add_argument("--compare-sequential", action="store_true", help="batched vs one launch per pattern")
     ap.add_argument("--autotune", action="store_true", help="with --compare-sequential: sweep launch configs")
     ap.add_argument("--ref-gpu-table", action="store_true",

@@ -283,7 +283,14 @@ typedef struct {
                                src/gpu_match.cu:302,316)                    */
   int32_t max_borrowed;     /* cap on the pool of borrowed arenas (0 = as
                                many as a quarter of free memory holds)       */
-  int32_t pad_;
+  int32_t prefetch_ahead;   /* paged, one plan: when a warp claims root chunk
+                               c (chunk = `chunk` roots in processing order),
+                               it posts the pages listed for chunk
+                               c + prefetch_ahead (0 = 2) to the copy ring  */
+  const int32_t* prefetch_off;   /* optional device ptr [prefetch_chunks+1]:
+                                    CSR offsets per chunk into prefetch_pages */
+  const int32_t* prefetch_pages; /* optional device ptr: page ids             */
+  int64_t prefetch_chunks;  /* chunks the lists cover                         */
 } pm_run_opts;
 
 void pm_run_opts_default(pm_run_opts* o);
@@ -318,6 +325,7 @@ typedef struct {
                                above it                                      */
   uint64_t prefix_cycles;   /* ... recomputing the path prefix of a donated
                                range (the cost of moving work between warps) */
+  uint64_t prefetch_requests; /* pages posted from the prefetch lists          */
 } pm_stats;
 
 /* Replaces the `_parallel_match` launch and the host reduction of per-warp

@@ -66,7 +66,8 @@ class RunOpts(C.Structure):
                 ("high_occupancy", C.c_int32), ("leaf_per_lane", C.c_int32), ("lane_subtree_max", C.c_int32),
                 ("root_counts", C.c_void_p), ("root_cost", C.c_void_p), ("root_order", C.c_void_p),
                 ("root_reads", C.c_void_p), ("own_arena_words", C.c_int64), ("max_borrowed", C.c_int32),
-                ("pad_", C.c_int32)]
+                ("prefetch_ahead", C.c_int32), ("prefetch_off", C.c_void_p), ("prefetch_pages", C.c_void_p),
+                ("prefetch_chunks", C.c_int64)]
 
 
 class Stats(C.Structure):
@@ -78,7 +79,7 @@ class Stats(C.Structure):
                 ("arena_bytes", C.c_uint64), ("device_status", C.c_uint32), ("pad_", C.c_uint32),
                 ("warp_ns", C.c_uint64), ("idle_ns", C.c_uint64), ("borrowed_arenas", C.c_uint64),
                 ("arena_pool", C.c_uint64), ("leaf_cycles", C.c_uint64), ("level_cycles", C.c_uint64),
-                ("prefix_cycles", C.c_uint64)]
+                ("prefix_cycles", C.c_uint64), ("prefetch_requests", C.c_uint64)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_ if not k.endswith("_")}
@@ -468,9 +469,9 @@ class Context:
         Keyword arguments are pm_run_opts fields (truncate, warps_per_block,
         chunk, split_level1, shard_rank/shard_count, root_begin/root_end,
         timeout_ms, cold_cache, high_occupancy, leaf_per_lane, lane_subtree_max, use_graph,
-        own_arena_words, max_borrowed) and
+        own_arena_words, max_borrowed, prefetch_ahead, prefetch_chunks) and
         device pointers root_counts_ptr, root_cost_ptr, root_order_ptr,
-        root_reads_ptr."""
+        root_reads_ptr, prefetch_off_ptr, prefetch_pages_ptr."""
         o = self._opts(**kw)
         k = len(patterns)
         arr = (C.c_void_p * k)(*[p._h.value for p in patterns])

@@ -71,6 +71,18 @@ __device__ __forceinline__ unsigned lanemask_lt() {
   return m;
 }
 
+// Publication of a donated item: the donor's release store of the slot's
+// sequence number orders its item writes before it; the taker's acquire load
+// orders its item reads after it.
+__device__ __forceinline__ void st_release(unsigned long long* p, unsigned long long v) {
+  asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ unsigned long long ld_acquire(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+
 struct MatchArgs {
   const uint64_t* rowptr;
   const int32_t* colidx;        // HBM residency
@@ -124,6 +136,12 @@ struct MatchArgs {
   unsigned long long timeout_ns;  // hard limit on the launch; idle warps also give
                                   // up after this long without a heartbeat
   DPaging pg;
+  // prefetch (paged, plan 0): pages to request for each root chunk, posted
+  // when the chunk pf_ahead chunks earlier is claimed (CSR over chunks)
+  const int32_t* pf_off;
+  const int32_t* pf_pages;
+  int32_t pf_ahead;
+  int32_t pf_chunks;
   // the launch's plans, in the kernel's own parameter block: every launch
   // carries its own copy, so launches that overlap on a device (other
   // contexts, prepared queries, the allocation-free entry) never see each
@@ -133,7 +151,9 @@ struct MatchArgs {
 
 enum { ST_SETOPS = 0, ST_BYTES = 1, ST_ROOTS = 2, ST_SPLITS = 3, ST_HITS = 4, ST_MISSES = 5,
        ST_ZC_BYTES = 6, ST_REQUESTS = 7, ST_EVICTIONS = 8, ST_DROPPED = 9, ST_WARP_NS = 10, ST_IDLE_NS = 11,
-       ST_BORROWS = 12, ST_LEAF_CYC = 13, ST_LEVEL_CYC = 14, ST_PREFIX_CYC = 15 };
+       ST_BORROWS = 12, ST_LEAF_CYC = 13, ST_LEVEL_CYC = 14, ST_PREFIX_CYC = 15, ST_PREFETCH = 16 };
+// control block words: cursors[32] counts[32] stats[kStatWords] status/active ...
+constexpr int kStatWords = 24;
 
 #define PM_SB_MAX 512      // ints of a leaf batch's common operand kept in shared memory
 #define PM_LANE_MAX 96     // longest first operand one lane handles alone in a leaf batch
@@ -164,7 +184,7 @@ struct WarpState {
 
 // Per-warp work counters (registers; flushed once at kernel exit).
 struct Work {
-  unsigned long long setops, bytes, reads, borrows;
+  unsigned long long setops, bytes, reads, borrows, prefetched;
   unsigned long long leaf_cyc, level_cyc, prefix_cyc;  // SM cycles by phase (lane 0's clock)
   unsigned int err;
   PageCounters pc;
@@ -426,10 +446,11 @@ __device__ int run_slot(const MatchArgs& a, const DPlan& P, WarpState& S, int L,
   if (!last && !slot_room(a, S, top, (T && scan > T) ? T : scan, w)) scan = 0;
   int32_t* out = S.arena + top;
   const uint32_t mask = P.slot_labels[s];
-  // an intersection whose second operand is not in shared memory and not
-  // much longer than the scanned part of the first: merge, B streamed through
-  // shared memory in coalesced windows; else a search per element of A
-  const bool merge = kind == SLOT_INTERSECT && B != S.sb && lenB > PM_WIN && (long long)lenB <= 32ll * scan;
+  // an intersection whose second operand is not in shared memory and at
+  // most 4x the scanned part of the first: merge, B streamed through shared
+  // memory in coalesced windows; else a search per element of A (which reads
+  // less of a much longer B)
+  const bool merge = kind == SLOT_INTERSECT && B != S.sb && lenB > PM_WIN && (long long)lenB <= 4ll * scan;
   int bpos = 0;  // merge: B[0, bpos) is below every element still to come
   for (int base = 0; base < scan; base += 32) {
     const int i = base + lane;
@@ -727,6 +748,11 @@ template <bool LABELED, int MODE>
 __device__ __forceinline__ unsigned leaf_walk(const MatchArgs& a, const WarpState& S, const LeafSet& m, int lenB,
                                               uint32_t mask, int t, int tend) {
   unsigned k = 0;
+  auto test = [&](int x) {
+    bool hit = leaf_member<MODE>(m, lenB, x);
+    if (LABELED && hit) hit = (mask >> a.labels[x]) & 1u;
+    k += hit ? 1u : 0u;
+  };
   int j = 0;  // the last candidate whose offset is <= t
 #pragma unroll
   for (int step = 16; step; step >>= 1)
@@ -736,24 +762,22 @@ __device__ __forceinline__ unsigned leaf_walk(const MatchArgs& a, const WarpStat
     const int stop = min(tend, S.lexcl[j + 1]);
     const int32_t* src = a.colidx + S.lrb[j] + (unsigned long long)(t - jbeg);
     const int n = stop - t;
-    int q = 0;
-    for (; q + 4 <= n; q += 4) {
-      int x[4];
-#pragma unroll
-      for (int u = 0; u < 4; u++) x[u] = src[q + u];
-#pragma unroll
-      for (int u = 0; u < 4; u++) {
-        bool hit = leaf_member<MODE>(m, lenB, x[u]);
-        if (LABELED && hit) hit = (mask >> a.labels[x[u]]) & 1u;
-        k += hit ? 1u : 0u;
-      }
+    // scalar up to a 16-byte boundary, then 128-bit loads, two in flight
+    int q = min(n, (int)((4 - ((reinterpret_cast<uintptr_t>(src) >> 2) & 3)) & 3));
+    for (int u = 0; u < q; u++) test(__ldg(src + u));
+    const int4* v = reinterpret_cast<const int4*>(src + q);
+    const int nv = (n - q) >> 2;
+    int i = 0;
+    for (; i + 2 <= nv; i += 2) {
+      const int4 a0 = __ldg(v + i), a1 = __ldg(v + i + 1);
+      test(a0.x); test(a0.y); test(a0.z); test(a0.w);
+      test(a1.x); test(a1.y); test(a1.z); test(a1.w);
     }
-    for (; q < n; q++) {
-      const int x = src[q];
-      bool hit = leaf_member<MODE>(m, lenB, x);
-      if (LABELED && hit) hit = (mask >> a.labels[x]) & 1u;
-      k += hit ? 1u : 0u;
+    if (i < nv) {
+      const int4 a0 = __ldg(v + i);
+      test(a0.x); test(a0.y); test(a0.z); test(a0.w);
     }
+    for (q += 4 * nv; q < n; q++) test(__ldg(src + q));
     t = stop;
     j++;
   }
@@ -1223,8 +1247,7 @@ __device__ __forceinline__ void maybe_donate(const MatchArgs& a, WarpState& S, i
         dst[0] = make_int4(plan_id, root_id, k, mid);
         dst[1] = make_int4(iend, S.path[2], S.path[3], S.path[4]);
         dst[2] = make_int4(S.path[5], S.path[6], 0, 0);
-        __threadfence();
-        atomicExch(&a.don_ready[slot & a.don_mask], slot + 1);
+        st_release(&a.don_ready[slot & a.don_mask], slot + 1);
         atomicAdd(&a.stats[ST_SPLITS], 1ull);
         S.iend[k] = mid;
         break;
@@ -1346,16 +1369,16 @@ __device__ bool take_donation(const MatchArgs& a, Donation& d) {
     const unsigned long long tail = *((volatile unsigned long long*)a.don_tail);
     const unsigned long long head = *((volatile unsigned long long*)a.don_head);
     if (tail < head) {
+      // counted as active before claiming (no fence: if another warp reads
+      // the claim before the count it may leave early, never lose work)
       atomicAdd(a.active, 1u);
-      __threadfence();
       if (atomicCAS(a.don_tail, tail, tail + 1) == tail) {
         // bounded wait for the donor to finish writing this slot
         for (int spin = 0; spin < (1 << 22); spin++) {
-          if (*((volatile unsigned long long*)&a.don_ready[tail & a.don_mask]) == tail + 1) { got = 1; break; }
+          if (ld_acquire(&a.don_ready[tail & a.don_mask]) == tail + 1) { got = 1; break; }
           __nanosleep(64);
         }
         if (got) {
-          __threadfence();
           const volatile int* src = (const volatile int*)(a.don_items + 3 * (tail & a.don_mask));
           for (int i = 0; i < 12; i++) v[i] = src[i];
         } else {
@@ -1428,6 +1451,25 @@ __global__ void __launch_bounds__(MINB == 1 ? 512 : 256, MINB) match_kernel(cons
       continue;
     }
     exhausted = 0;
+    if (PAGED && a.pf_off && p == 0) {
+      // post the predicted pages of a chunk this warp's successors will reach
+      const long long pc = (long long)gc + (long long)a.pf_ahead * a.shard_count;
+      if (pc < a.pf_chunks) {
+        PageCounters lpc = {};
+        for (int k = a.pf_off[pc] + lane; k < a.pf_off[pc + 1]; k += 32) {
+          const int32_t pg = a.pf_pages[k];
+          if (pg >= 0 && pg < a.pg.n_pages && ld_vol(&a.pg.page_frame[pg]) == PAGE_ABSENT) request_page(a.pg, pg, lpc);
+        }
+        unsigned long long v[3] = {lpc.requests, lpc.evictions, lpc.dropped};
+#pragma unroll
+        for (int q = 0; q < 3; q++)
+          for (int o = 16; o; o >>= 1) v[q] += __shfl_xor_sync(FULL, v[q], o);
+        w.pc.requests += v[0];
+        w.pc.evictions += v[1];
+        w.pc.dropped += v[2];
+        w.prefetched += v[0];
+      }
+    }
     const long long rb = (long long)gc * a.chunk;
     const long long re = min((long long)P.nroots, rb + a.chunk);
     unsigned long long local = 0;
@@ -1480,7 +1522,8 @@ __global__ void __launch_bounds__(MINB == 1 ? 512 : 256, MINB) match_kernel(cons
           if (a.root_cost) atomicAdd(&a.root_cost[item.root], (float)(w.bytes - b0));
           if (a.root_reads) atomicAdd(&a.root_reads[item.root], (float)(w.reads - r0));
         }
-        __threadfence();
+        // no fence: a warp that reads this decrement before this warp's
+        // donations can only leave early; this warp drains them itself
         atomicSub(a.active, 1u);
       }
       __syncwarp();
@@ -1524,6 +1567,7 @@ __global__ void __launch_bounds__(MINB == 1 ? 512 : 256, MINB) match_kernel(cons
     atomicAdd(&a.stats[ST_LEAF_CYC], w.leaf_cyc);
     atomicAdd(&a.stats[ST_LEVEL_CYC], w.level_cyc);
     atomicAdd(&a.stats[ST_PREFIX_CYC], w.prefix_cyc);
+    if (w.prefetched) atomicAdd(&a.stats[ST_PREFETCH], w.prefetched);
     if (PAGED) {
       atomicAdd(&a.stats[ST_HITS], w.pc.hits);
       atomicAdd(&a.stats[ST_MISSES], w.pc.misses);
@@ -2142,7 +2186,7 @@ static constexpr unsigned kDonSlots = 1u << 15;
 static constexpr int64_t kOwnSlotWords = 1 << 16;
 static constexpr int64_t kOwnGatherWords = 1 << 15;
 static constexpr size_t kBigPoolMaxBytes = 48ull << 30;
-static constexpr int kCtlRead = 32 + 32 + 16 + 1;  // cursors, counts, stats, status word
+static constexpr int kCtlRead = 32 + 32 + kStatWords + 1;  // cursors, counts, stats, status word
 
 // Validates the plans and options, builds the root lists into *roots,
 // sizes the persistent grid and the arenas, and fills L.  Buffers are grown
@@ -2264,7 +2308,7 @@ static pm_status setup_launch(pm_ctx* c, const pm_graph* g, const pm_plan* const
   L->big_bytes = big_bytes;
   // control block: cursors[32] counts[32] stats[16] status/active head tail
   // heartbeat, donation ready[] and items[]
-  L->ctl_words = 32 + 32 + 16 + 8 + kDonSlots + 6 * kDonSlots;
+  L->ctl_words = 32 + 32 + kStatWords + 8 + kDonSlots + 6 * kDonSlots;
   st = ensure((void**)ctl, ctl_bytes, L->ctl_words * 8);
   if (st != PM_OK) return st;
 
@@ -2290,7 +2334,7 @@ static pm_status setup_launch(pm_ctx* c, const pm_graph* g, const pm_plan* const
   unsigned long long* w = *ctl;
   a.cursors = w; w += 32;
   a.counts = w; w += 32;
-  a.stats = w; w += 16;
+  a.stats = w; w += kStatWords;
   a.status = (unsigned int*)w;
   a.active = (unsigned int*)w + 1; w += 1;
   a.don_head = w; w += 1;
@@ -2314,6 +2358,15 @@ static pm_status setup_launch(pm_ctx* c, const pm_graph* g, const pm_plan* const
   a.root_reads = o.root_reads;
   a.root_order = o.root_order;
   a.timeout_ns = (unsigned long long)(o.timeout_ms > 0 ? o.timeout_ms : 600000) * 1000000ull;
+  if (o.prefetch_off || o.prefetch_pages || o.prefetch_chunks) {
+    if (!L->paged) return fail(PM_ERR_INVALID, "prefetch lists need a paged graph");
+    if (nplans != 1 || !o.prefetch_off || !o.prefetch_pages || o.prefetch_chunks < 0)
+      return fail(PM_ERR_INVALID, "prefetch lists need one plan, both arrays and a chunk count");
+    a.pf_off = o.prefetch_off;
+    a.pf_pages = o.prefetch_pages;
+    a.pf_chunks = o.prefetch_chunks;
+    a.pf_ahead = o.prefetch_ahead > 0 ? o.prefetch_ahead : 2;
+  }
   for (int i = 0; i < nplans; i++) a.plans[i] = L->dp[i];
   L->active0 = (unsigned int)L->warps;
   if (L->paged) {
@@ -2345,7 +2398,7 @@ static pm_status enqueue_launch(pm_ctx* c, Launch& L, const unsigned int* active
 // Turns the read-back control words into counts, stats and a status.
 static pm_status finish_launch(const Launch& L, const unsigned long long* host_ctl, float kernel_ms, float roots_ms,
                                const pm_stats& pst, uint64_t* counts_out, pm_stats* stats_out) {
-  const unsigned int status = (unsigned int)(host_ctl[80] & 0xffffffffu);
+  const unsigned int status = (unsigned int)(host_ctl[64 + kStatWords] & 0xffffffffu);
   for (int i = 0; i < L.nplans; i++) {
     const Plan& p = *L.plans[i];
     counts_out[i] = host_ctl[32 + i] * (p.labeled ? 1ull : (uint64_t)p.multiplicity);
@@ -2373,6 +2426,7 @@ static pm_status finish_launch(const Launch& L, const unsigned long long* host_c
     so.leaf_cycles = stt[ST_LEAF_CYC];
     so.level_cycles = stt[ST_LEVEL_CYC];
     so.prefix_cycles = stt[ST_PREFIX_CYC];
+    so.prefetch_requests = stt[ST_PREFETCH];
     so.arena_pool = (uint64_t)L.n_big;
     so.device_status = status;
   }
@@ -2534,7 +2588,7 @@ static __device__ __align__(256) unsigned char g_static_scratch[PM_STATIC_SCRATC
 
 namespace {
 constexpr unsigned kStaticRing = 4096;  // donation slots inside the static scratch
-constexpr size_t kStaticCtlWords = 32 + 32 + 16 + 8 + kStaticRing + 6 * kStaticRing;
+constexpr size_t kStaticCtlWords = 32 + 32 + kStatWords + 8 + kStaticRing + 6 * kStaticRing;
 
 struct StaticScratch {
   bool ready = false;
@@ -2692,7 +2746,7 @@ extern "C" pm_status pm_match_static(const uint64_t* d_rowptr, const int32_t* d_
   unsigned long long* w = ctl;
   a.cursors = w; w += 32;
   a.counts = w; w += 32;
-  a.stats = w; w += 16;
+  a.stats = w; w += kStatWords;
   a.status = (unsigned int*)w;
   a.active = (unsigned int*)w + 1; w += 1;
   a.don_head = w; w += 1;

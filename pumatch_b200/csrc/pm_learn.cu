@@ -221,30 +221,58 @@ __global__ void quantize_kernel(const float* __restrict__ w, __nv_bfloat16* __re
 // ---------------------------------------------------------------- features
 // 16 features of a root edge (v0, v1); f[15] depends on the plan (how many
 // neighbours of v1 carry pattern vertex 2's label, as a fraction of deg v1).
+// What the first two levels of a root's DFS will see, for the cost features:
+// v2's candidates are v1's neighbours with v2's label (labeled) or below v0
+// (unlabeled, when the plan bounds v2 by v0); each contributes its neighbours
+// with v3's label (the label-group offsets give them directly) or its degree.
+struct FeatPlan {
+  int lab2, lab3;      // pattern labels of v2 and v3 (labeled; -1 when absent)
+  int bound_v0;        // unlabeled: v2 < v0
+  int nl1;             // label-group stride of lab_off, 0 without groups
+  const int32_t* lab_off;
+};
+
 __global__ void features_kernel(const uint64_t* __restrict__ rowptr, const int32_t* __restrict__ colidx,
                                 const uint8_t* __restrict__ labels, const int32_t* __restrict__ maxnbrdeg,
-                                const float* __restrict__ deg_rank, int nlabels, int lab2, const int2* roots,
+                                const float* __restrict__ deg_rank, int nlabels, FeatPlan fp, const int2* roots,
                                 int64_t nroots, float* __restrict__ out) {
+  const int lab2 = fp.lab2;
   const int lane = threadIdx.x & 31;
   const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
   for (int64_t r = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); r < nroots; r += warps) {
     const int2 e = roots[r];
     const uint64_t b1 = rowptr[e.y], e1 = rowptr[e.y + 1];
-    float two_hop = 0.f;
+    float two_hop = 0.f, pairs = 0.f;
     int hist[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    int match2 = 0;
+    int match2 = 0, cand2 = 0;
     for (uint64_t i = b1 + lane; i < e1; i += 32) {
       const int u = colidx[i];
-      two_hop += (float)(rowptr[u + 1] - rowptr[u]);
+      const float du = (float)(rowptr[u + 1] - rowptr[u]);
+      two_hop += du;
+      bool is_cand;
       if (labels) {
         const int l = labels[u];
         hist[l & 7]++;
         match2 += (l == lab2);
+        is_cand = (l == lab2);
+      } else {
+        is_cand = !fp.bound_v0 || u < e.x;
+      }
+      if (is_cand) {
+        cand2++;
+        if (labels && fp.lab_off && fp.lab3 >= 0 && fp.lab3 < fp.nl1 - 1) {
+          const int32_t* o = fp.lab_off + (int64_t)u * fp.nl1;
+          pairs += (float)(o[fp.lab3 + 1] - o[fp.lab3]);
+        } else {
+          pairs += du;
+        }
       }
     }
     for (int o = 16; o; o >>= 1) {
       two_hop += __shfl_xor_sync(0xffffffffu, two_hop, o);
+      pairs += __shfl_xor_sync(0xffffffffu, pairs, o);
       match2 += __shfl_xor_sync(0xffffffffu, match2, o);
+      cand2 += __shfl_xor_sync(0xffffffffu, cand2, o);
 #pragma unroll
       for (int k = 0; k < 8; k++) hist[k] += __shfl_xor_sync(0xffffffffu, hist[k], o);
     }
@@ -254,8 +282,8 @@ __global__ void features_kernel(const uint64_t* __restrict__ rowptr, const int32
       float* f = out + r * NIN;
       f[0] = log2f(1.f + d0);
       f[1] = log2f(1.f + d1);
-      f[2] = labels ? (float)labels[e.x] / (float)max(nlabels, 1) : 0.f;
-      f[3] = labels ? (float)labels[e.y] / (float)max(nlabels, 1) : 0.f;
+      f[2] = log2f(1.f + (float)cand2);  // level 1's candidates (v2)
+      f[3] = log2f(1.f + pairs);         // (v2, v3) candidate pairs below them
       f[4] = log2f(1.f + two_hop);
       f[5] = log2f(1.f + (float)maxnbrdeg[e.y]);
       f[6] = deg_rank ? deg_rank[e.y] : 0.f;
@@ -452,9 +480,15 @@ extern "C" pm_status pm_root_features(pm_ctx* c, const pm_graph* g, const pm_pla
   }
   const Plan* pl = plan_of(p);
   const int32_t* colidx = g->residency == PM_RESIDENT_HBM ? g->d_colidx : g->h_colidx_dev;
+  FeatPlan fp;
+  fp.lab2 = pl->nnodes > 2 ? pl->vertex_label[2] : -1;
+  fp.lab3 = pl->nnodes > 3 ? pl->vertex_label[3] : -1;
+  fp.bound_v0 = !pl->labeled && (pl->partial[pl->level_begin[1]] & 1u);
+  fp.nl1 = g->d_lab_off ? g->nl1 : 0;
+  fp.lab_off = g->d_lab_off;
   if (e == cudaSuccess) {
-    features_kernel<<<4 * c->nsm, 256>>>(g->d_rowptr, colidx, g->d_labels, g->d_maxnbrdeg, rank, g->nlabels,
-                                         pl->nnodes > 2 ? pl->vertex_label[2] : 0, roots, n, d_features);
+    features_kernel<<<4 * c->nsm, 256>>>(g->d_rowptr, colidx, g->d_labels, g->d_maxnbrdeg, rank, g->nlabels, fp,
+                                         roots, n, d_features);
     e = cudaGetLastError();
   }
   cudaError_t s2 = cudaDeviceSynchronize();

@@ -3,13 +3,16 @@
 The model (pm_mlp_*, hand-written CUDA in csrc/pm_learn.cu) maps 16 features of
 a root edge to [log(1 + DFS bytes), log(1 + adjacency reads)] of its subtree.
 It is trained on what the plain method logs about itself (per-root cost and
-reads from an ordinary run) and then used two ways, neither of which can change
-a count:
+reads from an ordinary run) and then used three ways, none of which can
+change a count:
   * root binning: roots are processed heaviest-first (longest-processing-time
     order), so the tail of a launch is made of cheap roots;
   * page residency (paged graphs): pages are scored by the predicted reads of
     the roots whose first two vertices' lists live in them, and the frame pool
-    starts with the highest-scoring pages instead of the first ones.
+    starts with the highest-scoring pages instead of starting cold;
+  * prefetch during the run (paged graphs): each root chunk gets a list of the
+    pages its predicted-heaviest roots will read first, which the kernel posts
+    to the copy ring a few chunks ahead (prefetch_lists).
 The plain path is the fallback (no model) and the baseline that prediction
 error and speed are measured against.
 """
@@ -149,3 +152,68 @@ def page_scores(rowptr: np.ndarray, roots: np.ndarray, pred_reads: np.ndarray, p
         np.add.at(score, first, pred_reads)
         np.add.at(score, last.astype(np.int64), pred_reads)
     return score
+
+
+def prefetch_lists(rowptr: np.ndarray, colidx: np.ndarray, roots: np.ndarray, order: np.ndarray,
+                   pred_reads: np.ndarray, page_ints: int, chunk: int, per_chunk: int = 64,
+                   cand_filter=None) -> Tuple[np.ndarray, np.ndarray]:
+    """Pages to request ahead of each root chunk (the kernel posts chunk c's
+    list when a warp claims chunk c - prefetch_ahead), as CSR (off, pages).
+
+    Roots are taken in processing order (`order`, root ids), `chunk` per
+    chunk.  Within a chunk, roots are ranked by their predicted page touches
+    (`pred_reads`, per root id); each adds the pages of its two vertices'
+    lists, then the pages of the lists of its level-1 candidates (v1's
+    neighbours passing `cand_filter(v1, neighbours)`, default all), until the
+    chunk holds per_chunk distinct pages.  Chunks whose roots are predicted to
+    touch nothing get none."""
+    n_chunks = (len(order) + chunk - 1) // chunk
+    off = np.zeros(n_chunks + 1, dtype=np.int32)
+    pages = []
+
+    def list_pages(v):
+        b, e = int(rowptr[v]), int(rowptr[v + 1])
+        if e <= b:
+            return range(0)
+        return range(b // page_ints, (e - 1) // page_ints + 1)
+
+    for k in range(n_chunks):
+        ids = order[k * chunk:(k + 1) * chunk]
+        ranked = ids[np.argsort(-pred_reads[ids], kind="stable")]
+        got = []
+        seen = set()
+
+        def add(rng):
+            for pg in rng:
+                if pg not in seen:
+                    seen.add(pg)
+                    got.append(pg)
+                    if len(got) >= per_chunk:
+                        return True
+            return False
+
+        full = False
+        for r in ranked:
+            if pred_reads[r] <= 0:
+                break
+            v0, v1 = int(roots[r, 0]), int(roots[r, 1])
+            if add(list_pages(v0)) or add(list_pages(v1)):
+                full = True
+                break
+        if not full:
+            for r in ranked:
+                if pred_reads[r] <= 0:
+                    break
+                v1 = int(roots[r, 1])
+                nb = colidx[int(rowptr[v1]):int(rowptr[v1 + 1])]
+                if cand_filter is not None:
+                    nb = cand_filter(v1, nb)
+                for u in nb[:per_chunk]:
+                    if add(list_pages(int(u))):
+                        full = True
+                        break
+                if full:
+                    break
+        pages.extend(got)
+        off[k + 1] = len(pages)
+    return off, np.asarray(pages, dtype=np.int32)

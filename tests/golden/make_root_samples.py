@@ -60,8 +60,8 @@ SAMPLES = {
                                          seed=2, device=0),
                               labeled=True, n_labels=8, label_seed=102,
                               pattern=P.to_g(*P.cycle_tail(5, 2), P.seeded_labels(7, 8, 202)), perm_seed=7,
-                              budget=1e12, budget_kind="alg_bytes", est_probes=60, est_seed=11, max_looked=4000,
-                              query_probes=2000, extra_budget=2e10, extra_cap=1e10),
+                              budget=4e11, budget_kind="alg_bytes", est_probes=40, est_seed=11, max_looked=600,
+                              max_kept=6, query_probes=1000, extra_budget=5e9, extra_cap=3e9, max_extra=6),
 }
 
 
@@ -96,13 +96,16 @@ def choose(g, p, roots, spec):
             break
         so, by, _ = orc.estimate(g, p, roots[i:i + 1], probes=spec["est_probes"], seed=spec["est_seed"])
         cost = by if by_bytes else so
-        if total < spec["budget"] and cost <= spec["budget"]:
+        max_kept, max_extra = spec.get("max_kept", 1 << 30), spec.get("max_extra", 1 << 30)
+        if total < spec["budget"] and cost <= spec["budget"] and len(kept) < max_kept:
             kept.append((int(i), so))
             total += cost
-        elif xtotal < xb and so <= spec["extra_cap"]:
+        elif xtotal < xb and so <= spec["extra_cap"] and len(extra) < max_extra:
             extra.append((int(i), so, by))
             xtotal += so
-        if total >= spec["budget"] and xtotal >= xb:
+        kept_done = total >= spec["budget"] or len(kept) >= max_kept
+        extra_done = xtotal >= xb or len(extra) >= max_extra
+        if kept_done and extra_done:
             break
     return kept, extra, looked
 
@@ -130,6 +133,7 @@ def make(name, threads):
                  f"kept estimates sum to {spec['budget']:.0e}"),
         "n_labels": spec.get("n_labels", 0), "label_seed": spec.get("label_seed"),
         "n_roots_total": int(len(roots)), "roots_examined": looked,
+        "max_kept": spec.get("max_kept"), "max_extra": spec.get("max_extra"),
         "query_set_ops_estimate": so_total,
         "roots": [{"index": int(i), "v0": int(roots[i][0]), "v1": int(roots[i][1]), "raw_count": int(c),
                    "count": int(c) * mult, "set_ops_estimate": so}
