@@ -645,6 +645,7 @@ def run_learned(args, workload):
     chunk = 16
     pf_off, pf_pages = learn.prefetch_lists(hg.rowptr, hg.colidx, roots, order.cpu().numpy(), pred_reads, page_ints,
                                             chunk, per_chunk=args.prefetch_pages)
+    split = learn.split_thresholds(pred)
     pf_off_d = torch.from_numpy(pf_off).cuda()
     pf_pages_d = torch.from_numpy(pf_pages if len(pf_pages) else np.zeros(1, dtype=np.int32)).cuda()
     kw = dict(timeout_ms=args.timeout_s * 1000, chunk=chunk)
@@ -652,7 +653,8 @@ def run_learned(args, workload):
         "plain": dict(cold_cache=1),
         "learned_residency_order": dict(root_order_ptr=order.data_ptr()),
         "learned": dict(root_order_ptr=order.data_ptr(), prefetch_off_ptr=pf_off_d.data_ptr(),
-                        prefetch_pages_ptr=pf_pages_d.data_ptr(), prefetch_chunks=len(pf_off) - 1),
+                        prefetch_pages_ptr=pf_pages_d.data_ptr(), prefetch_chunks=len(pf_off) - 1,
+                        root_split_ptr=split.data_ptr()),
     }
     hot = np.argsort(-score)[:info["n_frames"] - info["n_static_frames"]]
     res = {}
@@ -672,7 +674,8 @@ def run_learned(args, workload):
     line = {"metric": "query_ms_learned_vs_plain", "workload": workload, "count": count,
             "arms": res, "speedup": res["plain"]["kernel_ms"] / res["learned"]["kernel_ms"],
             "plain": "cold frame pool, CLOCK, reference root order",
-            "learned": "predicted-hot pages resident, heaviest-first roots, predicted pages prefetched per chunk",
+            "learned": "predicted-hot pages resident, heaviest-first roots, predicted pages prefetched per chunk, "
+                       "finer donation for roots predicted heavy",
             "prediction_mae_log": mae, "constant_predictor_mae_log": base, "train_loss": [hist[0], hist[-1]],
             "train_s": train_s, "train_roots": int(x.shape[0]), "eval_roots": int(xe.shape[0]),
             "frames": int(info["n_frames"]), "pages": int(info["n_pages"]),

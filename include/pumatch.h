@@ -291,6 +291,11 @@ typedef struct {
                                     CSR offsets per chunk into prefetch_pages */
   const int32_t* prefetch_pages; /* optional device ptr: page ids             */
   int64_t prefetch_chunks;  /* chunks the lists cover                         */
+  const int32_t* root_split; /* optional device ptr [n_roots], one plan: per
+                                root, the fewest last-but-one-level
+                                candidates a warp hands to idle warps (the
+                                split_level1 of that root; learned: lower
+                                for roots predicted heavy)                   */
 } pm_run_opts;
 
 void pm_run_opts_default(pm_run_opts* o);
@@ -400,9 +405,10 @@ pm_status pm_mlp_set_weights(pm_mlp* m, const float* host_in);
  *  - Limits: one plan; n below 2^31; the root list plus one block of warp
  *    arenas (patterns' worst-case candidate sets, sized from max_degree)
  *    must fit the scratch, otherwise PM_ERR_INVALID says so; fewer warps run
- *    when the arenas only partly fit.  Per-root outputs, root orders, ranges
- *    and shards are not supported here (PM_ERR_INVALID); every other
- *    pm_run_opts field means what it means for pm_match.
+ *    when the arenas only partly fit.  Per-root inputs and outputs, root
+ *    orders, ranges, shards and prefetch lists are not supported here
+ *    (PM_ERR_INVALID); every other pm_run_opts field means what it means for
+ *    pm_match.
  *  - The first call on a device looks up the scratch's device address
  *    (cudaGetSymbolAddress) with that device current; make that first call
  *    before any stream capture.

@@ -67,7 +67,7 @@ class RunOpts(C.Structure):
                 ("root_counts", C.c_void_p), ("root_cost", C.c_void_p), ("root_order", C.c_void_p),
                 ("root_reads", C.c_void_p), ("own_arena_words", C.c_int64), ("max_borrowed", C.c_int32),
                 ("prefetch_ahead", C.c_int32), ("prefetch_off", C.c_void_p), ("prefetch_pages", C.c_void_p),
-                ("prefetch_chunks", C.c_int64)]
+                ("prefetch_chunks", C.c_int64), ("root_split", C.c_void_p)]
 
 
 class Stats(C.Structure):
@@ -471,7 +471,7 @@ class Context:
         timeout_ms, cold_cache, high_occupancy, leaf_per_lane, lane_subtree_max, use_graph,
         own_arena_words, max_borrowed, prefetch_ahead, prefetch_chunks) and
         device pointers root_counts_ptr, root_cost_ptr, root_order_ptr,
-        root_reads_ptr, prefetch_off_ptr, prefetch_pages_ptr."""
+        root_reads_ptr, prefetch_off_ptr, prefetch_pages_ptr, root_split_ptr."""
         o = self._opts(**kw)
         k = len(patterns)
         arr = (C.c_void_p * k)(*[p._h.value for p in patterns])

@@ -124,6 +124,7 @@ struct MatchArgs {
   float* root_cost;
   float* root_reads;
   const int32_t* root_order;
+  const int32_t* root_split;      // optional per-root donation threshold of the last-but-one level (plan 0)
   // donation ring: items (plan, root, level, begin, end, path[2..level])
   int4* don_items;                // 3 int4 per slot
   unsigned long long* don_head;   // next slot to fill
@@ -160,7 +161,7 @@ constexpr int kStatWords = 24;
 #define PM_LEAF_BATCH 512  // candidates per leaf batch
 #define PM_WIN 256         // window of a merged second operand held in shared memory
 
-struct WarpState {
+struct alignas(16) WarpState {
   int32_t path[8];
   int32_t iter[8];
   int32_t iend[8];   // exclusive end of the iteration range per level
@@ -175,8 +176,12 @@ struct WarpState {
   int64_t cap;                   // slot words at `arena`
   int32_t ghalf;                 // words in each of the two gather halves (first and second operand)
   int32_t big;                   // borrowed arena, or -1
+  int32_t split;                 // donation threshold of the last-but-one level for the current root
   int32_t pins[PM_MAX_LIST_PAGES];  // paged mode: frames pinned for a gather
-  int32_t sb[PM_SB_MAX];            // leaf batches: the common operand (bitmap, hash table or sorted copy)
+  alignas(16) int32_t sb[PM_SB_MAX + 4];  // the common operand (bitmap, hash table or sorted copy); +4 for a
+                                         // bulk copy that starts up to 3 words before it
+  unsigned long long mbar;               // completion barrier of the warp's bulk copies
+  uint32_t mphase;                       // its current phase
   int32_t wb[PM_WIN];               // intersections by merge: the current window of the second operand
   unsigned long long lrb[32];       // leaf batches: start of each candidate's first operand in colidx
   int32_t lexcl[33];                // leaf batches: offset of each candidate's operand in the flat layout
@@ -262,6 +267,51 @@ __device__ __forceinline__ ListRef adj_label(const MatchArgs& a, WarpState& S, i
   w.reads++;
   if (!PAGED) return ListRef{a.colidx_lab + b + r.x, r.y, -1};
   return paged_list(a.pg, b + (uint64_t)r.x, r.y, gather, S.pins, w.pc);
+}
+
+// Stages n <= PM_SB_MAX words of the warp's arena into S.sb with one bulk
+// asynchronous copy (cp.async.bulk, completion counted in bytes on the warp's
+// mbarrier) and returns where src[0] landed: the copy starts at src rounded
+// down to 16 bytes and covers whole 16-byte units, which stay inside the
+// arena's allocation (every arena allocation has at least 256 bytes of slack
+// after its last word).  The wait is bounded: a copy not complete after
+// ~2^20 polls returns src itself (the caller reads B from global memory and
+// reports DEV_TIMEOUT).
+__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __noinline__ const int32_t* stage_bulk(WarpState& S, const int32_t* src, int n) {
+  const int lane = lane_id();
+  const uintptr_t sa = reinterpret_cast<uintptr_t>(src);
+  const uintptr_t a0 = sa & ~(uintptr_t)15;
+  const int head = (int)((sa - a0) >> 2);
+  const uint32_t bytes = (uint32_t)(((head + n) * 4 + 15) & ~15);
+  const uint32_t mbar = smem_addr(&S.mbar);
+  const uint32_t phase = S.mphase;
+  // the lanes' earlier generic writes of the slot (global) and accesses of
+  // S.sb (shared) come before the asynchronous proxy's read and write
+  asm volatile("fence.proxy.async;" ::: "memory");
+  __syncwarp();
+  if (lane == 0) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar), "r"(bytes) : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_addr(S.sb)),
+                 "l"(a0), "r"(bytes), "r"(mbar)
+                 : "memory");
+  }
+  uint32_t done = 0;
+  for (int spin = 0; spin < (1 << 20) && !done; spin++) {
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(mbar), "r"(phase)
+        : "memory");
+  }
+  done = __all_sync(FULL, done);
+  __syncwarp();
+  if (!done) return src;
+  if (lane == 0) S.mphase = phase ^ 1u;
+  __syncwarp();
+  return S.sb + head;
 }
 
 // Borrows a worst-case arena for the rest of the current root: copies the
@@ -415,12 +465,15 @@ __device__ int run_slot(const MatchArgs& a, const DPlan& P, WarpState& S, int L,
   const bool cgA = RA.cg;
   bool cgB = RB.cg;
   // a parent slot small enough goes to shared memory for the per-lane searches
+  bool b_shared = false;
   if (kind == SLOT_INTERSECT && L > 1 && lenB <= PM_SB_MAX) {
-    __syncwarp();
-    for (int i = lane; i < lenB; i += 32) S.sb[i] = B[i];
-    __syncwarp();
-    B = S.sb;
-    cgB = false;
+    if (lenB > 0) {
+      const int32_t* Bs = stage_bulk(S, B, lenB);
+      b_shared = Bs != B;
+      if (!b_shared) w.err |= DEV_TIMEOUT;
+      B = Bs;
+      cgB = cgB && !b_shared;
+    }
   }
 
   // symmetry-breaking upper bound (unlabeled only, src/gpu_match.cu:426-458)
@@ -450,7 +503,7 @@ __device__ int run_slot(const MatchArgs& a, const DPlan& P, WarpState& S, int L,
   // most 4x the scanned part of the first: merge, B streamed through shared
   // memory in coalesced windows; else a search per element of A (which reads
   // less of a much longer B)
-  const bool merge = kind == SLOT_INTERSECT && B != S.sb && lenB > PM_WIN && (long long)lenB <= 4ll * scan;
+  const bool merge = kind == SLOT_INTERSECT && !b_shared && lenB > PM_WIN && (long long)lenB <= 4ll * scan;
   int bpos = 0;  // merge: B[0, bpos) is below every element still to come
   for (int base = 0; base < scan; base += 32) {
     const int i = base + lane;
@@ -919,10 +972,9 @@ __device__ unsigned long long leaf_batch(const MatchArgs& a, const DPlan& P, War
       !(LABELED && a.lab_off && __popc(mask) == 1))
     return leaf_flat<LABELED>(a, S, cand, b, e, B, lenB, mask, common_ub, self_ub, w);
   const int32_t* Bs = B;
-  if (kind == SLOT_INTERSECT && lenB <= PM_SB_MAX) {
-    for (int i = lane; i < lenB; i += 32) S.sb[i] = B[i];
-    __syncwarp();
-    Bs = S.sb;
+  if (kind == SLOT_INTERSECT && lenB <= PM_SB_MAX && lenB > 0) {
+    Bs = stage_bulk(S, B, lenB);
+    if (Bs == B) w.err |= DEV_TIMEOUT;
   }
   unsigned long long cnt = 0, bytes = 0, ops = 0;  // per lane
   PageCounters lpc = {};                           // per lane (paged residency)
@@ -1134,9 +1186,8 @@ __device__ unsigned long long lane_subtree(const MatchArgs& a, const DPlan& P, W
   const int p1 = P.parent[X];
   const int lenB1 = S.size[p1];
   const int32_t* B1 = arena + S.off[p1];
-  for (int i = lane; i < lenB1; i += 32) S.sb[i] = B1[i];
-  __syncwarp();
-  const int32_t* Bs = S.sb;
+  const int32_t* Bs = lenB1 > 0 ? stage_bulk(S, B1, lenB1) : B1;
+  if (lenB1 > 0 && Bs == B1) w.err |= DEV_TIMEOUT;
   const int32_t* cand = arena + S.off[P.level_begin[L]];
   unsigned long long cnt = 0, bytes = 0, ops = 0;
   const int i = b + lane;
@@ -1240,7 +1291,7 @@ __device__ __forceinline__ void maybe_donate(const MatchArgs& a, WarpState& S, i
         head - tail < (unsigned long long)a.don_mask) {
       for (int k = L0; k <= L; k++) {
         const int it = S.iter[k], iend = S.iend[k];
-        if (iend - it < ((k + 1 == n - 2) ? max(a.split_min, 2) : 2)) continue;
+        if (iend - it < ((k + 1 == n - 2) ? max(S.split, 2) : 2)) continue;
         const int mid = it + (iend - it) / 2;  // it < mid < iend
         const unsigned long long slot = atomicAdd(a.don_head, 1ull);
         int4* dst = a.don_items + 3 * (slot & a.don_mask);
@@ -1429,6 +1480,9 @@ __global__ void __launch_bounds__(MINB == 1 ? 512 : 256, MINB) match_kernel(cons
     S.gather = own + a.slot_words;
     S.ghalf = (int32_t)(a.gather_words / 2);
     S.big = -1;
+    S.mphase = 0;
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&S.mbar)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncwarp();
   Work w;
@@ -1477,7 +1531,11 @@ __global__ void __launch_bounds__(MINB == 1 ? 512 : 256, MINB) match_kernel(cons
       const long long rid = a.root_order ? (long long)a.root_order[r] : r;
       const int2 e = P.roots[rid];
       const unsigned long long b0 = w.bytes, r0 = w.reads;
-      if (lane == 0) { S.path[0] = e.x; S.path[1] = e.y; }
+      if (lane == 0) {
+        S.path[0] = e.x;
+        S.path[1] = e.y;
+        S.split = (a.root_split && p == 0) ? a.root_split[rid] : a.split_min;
+      }
       __syncwarp();
       const unsigned long long c0 = dfs_from<LABELED, PAGED>(a, P, S, 1, 0, -1, true, p, (int)rid, w);
       return_arena(a, S, own);
@@ -1509,6 +1567,7 @@ __global__ void __launch_bounds__(MINB == 1 ? 512 : 256, MINB) match_kernel(cons
         S.path[0] = e.x;
         S.path[1] = e.y;
         for (int k = 2; k <= item.level; k++) S.path[k] = item.path[k];
+        S.split = (a.root_split && item.plan == 0) ? a.root_split[item.root] : a.split_min;
       }
       __syncwarp();
       const unsigned long long b0 = w.bytes, r0 = w.reads;
@@ -2357,6 +2416,8 @@ static pm_status setup_launch(pm_ctx* c, const pm_graph* g, const pm_plan* const
   a.root_cost = o.root_cost;
   a.root_reads = o.root_reads;
   a.root_order = o.root_order;
+  if (o.root_split && nplans != 1) return fail(PM_ERR_INVALID, "root_split needs a single plan");
+  a.root_split = o.root_split;
   a.timeout_ns = (unsigned long long)(o.timeout_ms > 0 ? o.timeout_ms : 600000) * 1000000ull;
   if (o.prefetch_off || o.prefetch_pages || o.prefetch_chunks) {
     if (!L->paged) return fail(PM_ERR_INVALID, "prefetch lists need a paged graph");
@@ -2650,9 +2711,11 @@ extern "C" pm_status pm_match_static(const uint64_t* d_rowptr, const int32_t* d_
   pm_run_opts o;
   pm_run_opts_default(&o);
   if (opts) o = *opts;
-  if (o.root_counts || o.root_cost || o.root_reads || o.root_order || o.shard_count > 1 || o.root_begin >= 0 ||
-      o.root_end >= 0)
-    return fail(PM_ERR_INVALID, "pm_match_static: per-root outputs, root orders, ranges and shards are not supported");
+  if (o.root_counts || o.root_cost || o.root_reads || o.root_order || o.root_split || o.shard_count > 1 ||
+      o.root_begin >= 0 || o.root_end >= 0 || o.prefetch_off || o.prefetch_pages || o.prefetch_chunks)
+    return fail(PM_ERR_INVALID,
+                "pm_match_static: per-root inputs and outputs, root orders, ranges, shards and prefetch lists are not "
+                "supported");
   int dev = 0;
   CK(cudaGetDevice(&dev));
   if (dev < 0 || dev >= 64) return fail(PM_ERR_INVALID, "pm_match_static: device %d out of range", dev);
@@ -2681,7 +2744,7 @@ extern "C" pm_status pm_match_static(const uint64_t* d_rowptr, const int32_t* d_
   const size_t warp_bytes = (size_t)slot_words * 4;
   const size_t ctl_bytes = kStaticCtlWords * 8;
   const size_t min_arena = (size_t)wpb * warp_bytes;  // one block
-  if (ctl_bytes + 64 + min_arena > PM_STATIC_SCRATCH_BYTES)
+  if (ctl_bytes + 64 + min_arena + 256 > PM_STATIC_SCRATCH_BYTES)
     return fail(PM_ERR_INVALID,
                 "pm_match_static: one block of warp arenas needs %zu bytes, beyond the %llu-byte static scratch "
                 "(max degree %d is too large for this entry point)",
@@ -2691,7 +2754,7 @@ extern "C" pm_status pm_match_static(const uint64_t* d_rowptr, const int32_t* d_
   unsigned long long* rcount = (unsigned long long*)(base + ctl_bytes);
   int2* roots = (int2*)(base + ctl_bytes + 64);
   const size_t after_ctl = PM_STATIC_SCRATCH_BYTES - ctl_bytes - 64;
-  const unsigned long long root_cap = (after_ctl - min_arena) / sizeof(int2);
+  const unsigned long long root_cap = (after_ctl - min_arena - 256) / sizeof(int2);
 
   CK(cudaMemsetAsync(base, 0, ctl_bytes + 64, st));  // previous calls leave their contents behind
   const RootFilter f = to_filter(p);
@@ -2706,7 +2769,9 @@ extern "C" pm_status pm_match_static(const uint64_t* d_rowptr, const int32_t* d_
                 nroots, root_cap);
   const size_t roots_bytes = ((size_t)nroots * sizeof(int2) + 255) & ~(size_t)255;
   int32_t* arena = (int32_t*)((unsigned char*)roots + roots_bytes);
-  const size_t arena_bytes = after_ctl - roots_bytes;
+  // 256 bytes of slack after the last arena: bulk copies of a slot round its
+  // end up to 16 bytes
+  const size_t arena_bytes = after_ctl - roots_bytes - 256;
   // kernel variant by register cap, as pm_match chooses it
   int variant = o.high_occupancy;
   if (variant == 0) variant = (wpb <= 8) ? 2 : 3;

@@ -141,6 +141,20 @@ def heavy_first_order(pred):
     return torch.argsort(pred[:, 0], descending=True).to(torch.int32).contiguous()
 
 
+def split_thresholds(pred, base: int = 64, heavy_q: float = 0.9, light_q: float = 0.5):
+    """Per-root donation thresholds (int32 device tensor, root order) from the
+    predicted log cost: roots above the heavy quantile hand out their
+    last-but-one-level ranges from base/4 candidates on, roots below the light
+    quantile only from 2*base, the rest from base."""
+    import torch
+    c = pred[:, 0]
+    hi, lo = torch.quantile(c, heavy_q), torch.quantile(c, light_q)
+    out = torch.full_like(c, float(base))
+    out[c >= hi] = max(2, base // 4)
+    out[c < lo] = 2 * base
+    return out.to(torch.int32).contiguous()
+
+
 def page_scores(rowptr: np.ndarray, roots: np.ndarray, pred_reads: np.ndarray, page_ints: int, n_pages: int):
     """Predicted demand per adjacency page: each root adds its predicted reads
     to the pages holding its two vertices' lists."""

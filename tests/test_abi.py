@@ -152,8 +152,9 @@ int main(void){
         offsetof(pm_stats, idle_ns), offsetof(pm_run_opts, own_arena_words), offsetof(pm_run_opts, max_borrowed),
         offsetof(pm_stats, borrowed_arenas), offsetof(pm_stats, arena_pool), sizeof(pm_run_opts), sizeof(pm_stats));
  printf("%zu %zu %zu\n", offsetof(pm_stats, leaf_cycles), offsetof(pm_stats, level_cycles), offsetof(pm_stats, prefix_cycles));
- printf("%zu %zu %zu %zu %zu\n", offsetof(pm_run_opts, prefetch_ahead), offsetof(pm_run_opts, prefetch_off),
-        offsetof(pm_run_opts, prefetch_pages), offsetof(pm_run_opts, prefetch_chunks), offsetof(pm_stats, prefetch_requests));
+ printf("%zu %zu %zu %zu %zu %zu\n", offsetof(pm_run_opts, prefetch_ahead), offsetof(pm_run_opts, prefetch_off),
+        offsetof(pm_run_opts, prefetch_pages), offsetof(pm_run_opts, prefetch_chunks), offsetof(pm_stats, prefetch_requests),
+        offsetof(pm_run_opts, root_split));
  return 0; }'''
     import ctypes as C
     import tempfile
@@ -169,7 +170,7 @@ int main(void){
                     C.sizeof(pm.Stats), pm.Stats.leaf_cycles.offset, pm.Stats.level_cycles.offset,
                     pm.Stats.prefix_cycles.offset, pm.RunOpts.prefetch_ahead.offset, pm.RunOpts.prefetch_off.offset,
                     pm.RunOpts.prefetch_pages.offset, pm.RunOpts.prefetch_chunks.offset,
-                    pm.Stats.prefetch_requests.offset]
+                    pm.Stats.prefetch_requests.offset, pm.RunOpts.root_split.offset]
 
 
 def test_c_program_links_and_runs_host_entry_points(tmp_path):
