@@ -100,10 +100,10 @@ WORKLOADS = {
     # twenty seeded 4-7-vertex patterns in one persistent launch
     "rmat128k_batch20_lab32": dict(graph=_RMAT128K, labeled=True, n_labels=32, label_seed=102, batch_seed=303),
     # learned-scheduler comparison (--learned): trained on seeds 11, 12, 13;
-    # a frame pool of a quarter of the adjacency, all of it under CLOCK
+    # a frame pool of half the adjacency, all of it under CLOCK
     "rmat128k_c5t2_lab32_clock": dict(graph=_RMAT128K, labeled=True, n_labels=32, label_seed=102,
                                       pattern_label_seed=202, patterns=[("C5t2", P.cycle_tail(5, 2))],
-                                      paged=dict(frame_fraction=0.25, static_fraction=0.0, page_bytes=16 << 10)),
+                                      paged=dict(frame_fraction=0.5, static_fraction=0.0, page_bytes=16 << 10)),
     # the same graph with the reference's split: 60% of the adjacency in
     # static frames plus 28% evictable
     "rmat128k_c5t2_lab32_paged": dict(graph=_RMAT128K, labeled=True, n_labels=32, label_seed=102,
@@ -658,12 +658,15 @@ def run_learned(args, workload):
     }
     hot = np.argsort(-score)[:info["n_frames"] - info["n_static_frames"]]
     res = {}
+    print(f"learned: trained in {train_s:.1f} s on {int(x.shape[0])} roots; evaluating", file=sys.stderr, flush=True)
     for mode, extra in arms.items():
         g.set_resident_pages(hot if mode != "plain" else np.zeros(0, dtype=np.int64))
         times, stats = [], None
         for k in range(args.warmup + args.steps):
             c, stt = ctx.match(g, [p], **kw, **extra)
             assert c[0] == count, (mode, c, count)
+            print(f"  {mode} run {k}: {stt['kernel_ms']:.1f} ms, {stt['page_misses']} misses", file=sys.stderr,
+                  flush=True)
             if k >= args.warmup:
                 times.append(stt["kernel_ms"])
                 stats = stt

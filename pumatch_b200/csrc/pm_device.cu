@@ -269,6 +269,10 @@ __device__ __forceinline__ ListRef adj_label(const MatchArgs& a, WarpState& S, i
   return paged_list(a.pg, b + (uint64_t)r.x, r.y, gather, S.pins, w.pc);
 }
 
+// Operands shorter than this are staged by the lanes' own loads: a bulk
+// copy's round trip through the mbarrier costs more than a few loads.
+#define PM_BULK_MIN 256
+
 // Stages n <= PM_SB_MAX words of the warp's arena into S.sb with one bulk
 // asynchronous copy (cp.async.bulk, completion counted in bytes on the warp's
 // mbarrier) and returns where src[0] landed: the copy starts at src rounded
@@ -281,6 +285,12 @@ __device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)
 
 __device__ __noinline__ const int32_t* stage_bulk(WarpState& S, const int32_t* src, int n) {
   const int lane = lane_id();
+  if (n < PM_BULK_MIN) {
+    __syncwarp();
+    for (int i = lane; i < n; i += 32) S.sb[i] = src[i];
+    __syncwarp();
+    return S.sb;
+  }
   const uintptr_t sa = reinterpret_cast<uintptr_t>(src);
   const uintptr_t a0 = sa & ~(uintptr_t)15;
   const int head = (int)((sa - a0) >> 2);
@@ -845,8 +855,9 @@ __device__ __forceinline__ unsigned leaf_walk(const MatchArgs& a, const WarpStat
 // lists, four loads in flight, testing each element against B's structure in
 // shared memory (leaf_build).  Counts only; no truncation.  Same set
 // operations, counts and accounting as lane_intersect per candidate.
-// a.leaf_flat == 2 selects the earlier strided layout (element t0 + lane,
-// owner found per element by shuffles), kept for comparison.
+// Batches averaging under 16 elements per lane, and a.leaf_flat == 2, use
+// the strided layout instead (element t0 + lane, owner found per element by
+// shuffles): it has no per-lane setup per candidate.
 template <bool LABELED>
 __device__ unsigned long long leaf_flat(const MatchArgs& a, WarpState& S, const int32_t* cand, int b, int e,
                                         const int32_t* B, int lenB, uint32_t mask, int common_ub, bool self_ub,
@@ -875,7 +886,9 @@ __device__ unsigned long long leaf_flat(const MatchArgs& a, WarpState& S, const 
       if (lane >= o) incl += t;
     }
     const int total = __shfl_sync(FULL, incl, 31);
-    if (a.leaf_flat == 2) {
+    // short lists (under 16 elements per lane): the strided layout has no
+    // per-candidate setup per lane
+    if (a.leaf_flat == 2 || total < 16 * 32) {
       const int excl = incl - lenA;
       for (int t0 = 0; t0 < total; t0 += 32) {
         const int t = t0 + lane;
@@ -2334,6 +2347,8 @@ static pm_status setup_launch(pm_ctx* c, const pm_graph* g, const pm_plan* const
                         : (L->paged ? match_kernel<false, true, 1> : match_kernel<false, false, 1>);
   }
   int per_sm = 0;
+  // per-warp state is ~4 KB: 16-warp blocks need more than the default 48 KB
+  CK(cudaFuncSetAttribute(L->kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L->smem));
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, L->kfn, L->threads, L->smem));
   if (o.blocks_per_sm > 0) per_sm = std::min(per_sm, o.blocks_per_sm);
   per_sm = std::max(per_sm, 1);
@@ -2783,6 +2798,7 @@ extern "C" pm_status pm_match_static(const uint64_t* d_rowptr, const int32_t* d_
       : variant == 2 ? (p.labeled ? match_kernel<true, false, 3> : match_kernel<false, false, 3>)
                      : (p.labeled ? match_kernel<true, false, 1> : match_kernel<false, false, 1>);
   int per_sm = 0;
+  CK(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(sizeof(WarpState) * wpb)));
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, wpb * 32, sizeof(WarpState) * wpb));
   if (o.blocks_per_sm > 0) per_sm = std::min(per_sm, o.blocks_per_sm);
   int64_t blocks = std::max(1, per_sm) * (int64_t)nsm;

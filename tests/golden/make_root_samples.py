@@ -60,8 +60,9 @@ SAMPLES = {
                                          seed=2, device=0),
                               labeled=True, n_labels=8, label_seed=102,
                               pattern=P.to_g(*P.cycle_tail(5, 2), P.seeded_labels(7, 8, 202)), perm_seed=7,
-                              budget=4e11, budget_kind="alg_bytes", est_probes=40, est_seed=11, max_looked=600,
-                              max_kept=6, query_probes=1000, extra_budget=5e9, extra_cap=3e9, max_extra=6),
+                              budget=4e11, budget_kind="alg_bytes", est_probes=20, est_seed=11, max_looked=300,
+                              max_kept=6, query_probes=300, extra_budget=5e9, extra_cap=3e9, max_extra=6,
+                              verify_s=40.0),
 }
 
 
@@ -90,10 +91,14 @@ def choose(g, p, roots, spec):
     kept, extra, total, xtotal, looked = [], [], 0.0, 0.0, 0
     by_bytes = spec.get("budget_kind") == "alg_bytes"
     xb = spec.get("extra_budget", 0.0)
+    t0 = time.time()
     for i in perm:
         looked += 1
         if looked > spec["max_looked"]:
             break
+        if looked % 25 == 0:
+            print(f"  examined {looked} roots, kept {len(kept)}, extra {len(extra)}, {time.time() - t0:.0f} s",
+                  flush=True)
         so, by, _ = orc.estimate(g, p, roots[i:i + 1], probes=spec["est_probes"], seed=spec["est_seed"])
         cost = by if by_bytes else so
         max_kept, max_extra = spec.get("max_kept", 1 << 30), spec.get("max_extra", 1 << 30)
@@ -112,16 +117,42 @@ def choose(g, p, roots, spec):
 
 def make(name, threads):
     spec = SAMPLES[name]
+    t0 = time.time()
     rp, ci = build_graph(spec["graph"])
     labels = orc.gen_labels(len(rp) - 1, spec["n_labels"], spec["label_seed"]) if spec["labeled"] else None
     g = orc.Graph(rp, ci, labels)
     p = orc.plan(spec["pattern"], spec["labeled"])
+    print(f"{name}: graph {time.time() - t0:.0f} s", flush=True)
     roots = orc.roots(g, p)
+    print(f"{name}: {len(roots)} roots, {time.time() - t0:.0f} s", flush=True)
     kept, extra, looked = choose(g, p, roots, spec)
-    idx = np.array([i for i, _ in kept], dtype=np.int64)
-    t0 = time.time()
-    total, per_root, done, pieces, st = orc.count_split(g, p, roots[idx], threads=threads)
-    assert done == pieces
+    print(f"{name}: {len(kept)} kept, {len(extra)} extra of {looked} examined, {time.time() - t0:.0f} s", flush=True)
+    t1 = time.time()
+    if spec.get("verify_s"):
+        # exact counts within a time limit per root (a run whose pieces all
+        # finish is exact); a root the oracle cannot finish in time is timed
+        # on the GPU without a count
+        ok, counts = [], []
+        st = {"set_ops": 0, "alg_bytes": 0}
+        for i, so in kept:
+            c, _, done, pieces, s1 = orc.count_split(g, p, roots[i:i + 1], threads=threads,
+                                                     time_limit_s=spec["verify_s"])
+            if done == pieces:
+                ok.append((i, so))
+                counts.append(c)
+                st["set_ops"] += s1["set_ops"]
+                st["alg_bytes"] += s1["alg_bytes"]
+            else:
+                extra.append((i, so, float("nan")))
+            print(f"  root {i}: {'counted' if done == pieces else 'too slow for the oracle'}, "
+                  f"{time.time() - t0:.0f} s", flush=True)
+        kept = ok
+        per_root = np.array(counts, dtype=np.uint64)
+        total = int(per_root.sum())
+    else:
+        idx = np.array([i for i, _ in kept], dtype=np.int64)
+        total, per_root, done, pieces, st = orc.count_split(g, p, roots[idx], threads=threads)
+        assert done == pieces
     mult = 1 if spec["labeled"] else p.multiplicity
     so_total, _, _ = orc.estimate(g, p, roots, probes=spec["query_probes"], seed=spec["est_seed"])
     rec = {
@@ -139,12 +170,13 @@ def make(name, threads):
                    "count": int(c) * mult, "set_ops_estimate": so}
                   for (i, so), c in zip(kept, per_root)],
         "extra_roots": [{"index": int(i), "v0": int(roots[i][0]), "v1": int(roots[i][1]), "set_ops_estimate": so,
-                         "alg_bytes_estimate": by} for i, so, by in extra],
+                         "alg_bytes_estimate": None if by != by else by} for i, so, by in extra],
         "extra_rule": (f"the same permutation's roots whose estimate is at most {spec['extra_cap']:.0e} set "
-                       f"operations, until they sum to {spec['extra_budget']:.0e}; timed on the GPU, not counted "
-                       f"by the oracle") if extra else None,
+                       f"operations, until they sum to {spec['extra_budget']:.0e}, and candidates the oracle could "
+                       f"not count within {spec.get('verify_s')} s; timed on the GPU, not counted by the oracle")
+                      if extra else None,
         "raw_count": int(total), "count": int(total) * mult, "set_ops": int(st["set_ops"]),
-        "alg_bytes": int(st["alg_bytes"]), "oracle_s": round(time.time() - t0, 1), "oracle_threads": threads,
+        "alg_bytes": int(st["alg_bytes"]), "oracle_s": round(time.time() - t1, 1), "oracle_threads": threads,
     }
     return rec
 

@@ -56,8 +56,9 @@ def test_tiny_own_arenas_borrow_and_keep_counts(ctx, name, labeled, text, paged)
             got, st = ctx.match(g, [p], own_arena_words=own, timeout_ms=120000, **rng)
             assert got[0] == want, own
             assert st["set_ops"] == ost["set_ops"]
-            if ost["set_ops"] > 1000:
-                assert st["borrowed_arenas"] > 0 and st["arena_pool"] >= 1
+            assert st["arena_pool"] >= 1  # the own arena is below the plans' worst case
+            if name == "cl3000" and own == 48:  # sets that certainly outgrow 48 words
+                assert st["borrowed_arenas"] > 0
         # a pool of one arena: warps queue for it (every root needs it, so
         # the roots run one at a time -- a small range of them)
         k = 100 if paged else 300

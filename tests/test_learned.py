@@ -138,13 +138,12 @@ def test_gpu_learned_order_and_residency_keep_counts(ctx):
 @gpu
 def test_gpu_learned_scheduling_gains_over_plain(ctx):
     """What the trained network gains, on a fixed seed: a paged R-MAT graph
-    whose frame pool holds a quarter of the adjacency, all under CLOCK.  The
+    whose frame pool holds half of the adjacency, all under CLOCK.  The
     plain method starts cold and pages in on demand; the learned one starts
     with the pages the model (trained on three other seeds) predicts
     hottest, runs roots heaviest-first, prefetches each chunk's predicted
-    pages during the run and splits predicted-heavy roots more finely.  Counts are identical; the learned run misses less
-    and finishes sooner."""
-    import statistics
+    pages during the run and splits predicted-heavy roots more finely.
+    Counts are identical; the learned run misses less and finishes sooner."""
 
     import torch
 
@@ -154,7 +153,7 @@ def test_gpu_learned_scheduling_gains_over_plain(ctx):
     text = P.to_g(*P.cycle_tail(5, 2), P.seeded_labels(7, 32, 202))
 
     def graph(seed):
-        hg = pm.gen_rmat(1 << 16, 16 << 16, seed=seed)
+        hg = pm.gen_rmat(1 << 15, 16 << 15, seed=seed)
         return pm.HostGraph(hg.rowptr, hg.colidx, pm.gen_labels(hg.n, 32, seed=102 + 1000 * seed))
 
     xs, ts = [], []
@@ -171,7 +170,7 @@ def test_gpu_learned_scheduling_gains_over_plain(ctx):
     hg = graph(2)
     pb = 16 << 10
     g = pm.GraphPreprocessor.from_host(hg, labeled=True, paged=True, page_bytes=pb,
-                                       frame_pool_bytes=max(pb, hg.colidx.nbytes // 4 // pb * pb))
+                                       frame_pool_bytes=max(pb, hg.colidx.nbytes // 2 // pb * pb))
     p = pm.PatternPreprocessor(text=text, labeled=True)
     pred = m.predict(learn.root_features(ctx, g, p))
     # the prediction beats a constant one on the held-out seed
@@ -200,12 +199,12 @@ def test_gpu_learned_scheduling_gains_over_plain(ctx):
                       prefetch_pages_ptr=pages_d.data_ptr(), prefetch_chunks=len(off) - 1,
                       root_split_ptr=split.data_ptr())
         ms, misses = [], []
-        for _ in range(3):
+        for _ in range(2):
             c, st = ctx.match(g, [p], chunk=16, **kw)
             assert c[0] == count
             ms.append(st["kernel_ms"])
             misses.append(st["page_misses"])
-        res[mode] = (statistics.median(ms), statistics.median(misses))
+        res[mode] = (min(ms), min(misses))
     assert res["learned"][1] < res["plain"][1], res
     assert res["learned"][0] < res["plain"][0], res
     g.close()
