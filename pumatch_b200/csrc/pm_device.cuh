@@ -51,8 +51,10 @@ struct DPaging {
   int64_t n_pages;
   int64_t n_frames;
   int32_t* page_frame;             // [n_pages]: frame, or PAGE_ABSENT/LOADING/EVICTING
-  int32_t* frame_page;             // [n_frames]: page held, -1 never used
-  int32_t* frame_pin;              // [n_frames]: readers in flight
+  // [n_frames]: (page held << 32) | readers in flight; page all ones when
+  // never used.  One word, so a pin and an eviction are ordered by the word
+  // itself: an evictor's CAS needs zero pins, a reader's add sees the tag.
+  unsigned long long* frame_state;
   uint8_t* frame_ref;              // [n_frames]: CLOCK reference bits
   int32_t* frames;                 // [n_frames << page_shift]
   const int32_t* host_colidx;      // device-visible pointer to the paged host array

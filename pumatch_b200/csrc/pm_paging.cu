@@ -39,8 +39,7 @@ struct PagedState {
   int device = 0;
   int32_t* frames = nullptr;
   int32_t* page_frame = nullptr;
-  int32_t* frame_page = nullptr;
-  int32_t* frame_pin = nullptr;
+  unsigned long long* frame_state = nullptr;  // (page << 32) | pins per frame
   uint8_t* frame_ref = nullptr;
   unsigned long long* dctl = nullptr;  // [0] clock hand, [1] next free, [2] ring head
   // mapped pinned host memory
@@ -60,6 +59,7 @@ struct PagedState {
   int32_t* init_fp = nullptr;  // pinned [n_frames]: frame -> page at the start of a run
   int32_t* cold_pf = nullptr;  // pinned [n_pages]: the same for a cold run (static frames only)
   int32_t* cold_fp = nullptr;  // pinned [n_frames]
+  unsigned long long* fs_host = nullptr;  // pinned [n_frames]: frame states to upload
   // service thread
   std::thread th;
   std::atomic<bool> stop{false};
@@ -73,8 +73,7 @@ static void release_state(PagedState* s) {
   if (!s) return;
   cudaFree(s->frames);
   cudaFree(s->page_frame);
-  cudaFree(s->frame_page);
-  cudaFree(s->frame_pin);
+  cudaFree(s->frame_state);
   cudaFree(s->frame_ref);
   cudaFree(s->dctl);
   cudaFreeHost(s->ring);
@@ -85,6 +84,7 @@ static void release_state(PagedState* s) {
   cudaFreeHost(s->init_fp);
   cudaFreeHost(s->cold_pf);
   cudaFreeHost(s->cold_fp);
+  cudaFreeHost(s->fs_host);
   if (s->copy_stream) cudaStreamDestroy(s->copy_stream);
   delete s;
 }
@@ -99,7 +99,10 @@ static pm_status reset_table(pm_graph* g, cudaStream_t st, bool cold) {
   const int32_t* pf = cold ? s->cold_pf : s->init_pf;
   const int32_t* fp = cold ? s->cold_fp : s->init_fp;
   CKP(cudaMemcpyAsync(s->page_frame, pf, sizeof(int32_t) * g->n_pages, cudaMemcpyHostToDevice, st));
-  CKP(cudaMemcpyAsync(s->frame_page, fp, sizeof(int32_t) * g->n_frames, cudaMemcpyHostToDevice, st));
+  // every frame starts unpinned, tagged with the page it holds (all ones when empty)
+  for (int64_t f = 0; f < g->n_frames; f++) s->fs_host[f] = (unsigned long long)(uint32_t)fp[f] << 32;
+  CKP(cudaMemcpyAsync(s->frame_state, s->fs_host, sizeof(unsigned long long) * g->n_frames,
+                      cudaMemcpyHostToDevice, st));
   const size_t pb = (size_t)g->page_ints * 4;
   for (int64_t f = s->static_loaded ? s->n_static : 0; f < pre;) {
     // coalesce runs of consecutive pages in consecutive frames into one copy
@@ -111,7 +114,6 @@ static pm_status reset_table(pm_graph* g, cudaStream_t st, bool cold) {
     CKP(cudaMemcpyAsync((char*)s->frames + (size_t)f * pb, g->h_paged + first, bytes, cudaMemcpyHostToDevice, st));
     f = e;
   }
-  CKP(cudaMemsetAsync(s->frame_pin, 0, sizeof(int32_t) * g->n_frames, st));
   CKP(cudaMemsetAsync(s->frame_ref, 0, g->n_frames, st));
   unsigned long long h[4] = {0, (unsigned long long)pre, 0, 0};
   CKP(cudaMemcpyAsync(s->dctl, h, sizeof(h), cudaMemcpyHostToDevice, st));
@@ -180,8 +182,7 @@ pm_status paged_place(pm_graph* g, const int32_t* colidx, const pm_graph_opts* o
   const size_t fbytes = (size_t)g->n_frames * pb;
   CKP(cudaMalloc(&s->frames, std::max<size_t>(fbytes, 4)));
   CKP(cudaMalloc(&s->page_frame, sizeof(int32_t) * std::max<int64_t>(g->n_pages, 1)));
-  CKP(cudaMalloc(&s->frame_page, sizeof(int32_t) * std::max<int64_t>(g->n_frames, 1)));
-  CKP(cudaMalloc(&s->frame_pin, sizeof(int32_t) * std::max<int64_t>(g->n_frames, 1)));
+  CKP(cudaMalloc(&s->frame_state, sizeof(unsigned long long) * std::max<int64_t>(g->n_frames, 1)));
   CKP(cudaMalloc(&s->frame_ref, std::max<int64_t>(g->n_frames, 1)));
   CKP(cudaMalloc(&s->dctl, sizeof(unsigned long long) * 4));
   g->device_bytes += fbytes + 4 * g->n_pages + 9 * g->n_frames;
@@ -204,6 +205,7 @@ pm_status paged_place(pm_graph* g, const int32_t* colidx, const pm_graph_opts* o
   CKP(cudaHostAlloc((void**)&s->init_fp, fpb, cudaHostAllocPortable));
   CKP(cudaHostAlloc((void**)&s->cold_pf, pfb, cudaHostAllocPortable));
   CKP(cudaHostAlloc((void**)&s->cold_fp, fpb, cudaHostAllocPortable));
+  CKP(cudaHostAlloc((void**)&s->fs_host, 2 * fpb, cudaHostAllocPortable));
   s->n_static = s->n_static_cap = std::min<int64_t>((int64_t)(o->static_pool_bytes / pb), g->n_frames);
   g->ps = s.release();
   std::vector<int64_t> prefix((size_t)g->n_frames);
@@ -246,8 +248,7 @@ pm_status paged_prepare(pm_ctx* c, pm_graph* g, bool cold, DPaging* out) {
   out->n_pages = g->n_pages;
   out->n_frames = g->n_frames;
   out->page_frame = s->page_frame;
-  out->frame_page = s->frame_page;
-  out->frame_pin = s->frame_pin;
+  out->frame_state = s->frame_state;
   out->frame_ref = s->frame_ref;
   out->frames = s->frames;
   out->host_colidx = g->h_paged_dev;

@@ -9,9 +9,10 @@
 //     fixed power-of-two range of it; a device frame pool caches pages;
 //   * page_frame[page] is the device-resident page table (frame index, or
 //     ABSENT / LOADING / EVICTING);
-//   * a warp that finds a list resident pins its frame, re-checks the
-//     mapping and reads the frame; a list spanning several pages is gathered
-//     into the warp's arena when all its pages are resident;
+//   * a warp that finds a list resident pins its frame (one acquire add on
+//     the frame's (page, pins) word, no fence), re-checks the mapping and
+//     reads the frame; a list spanning several pages is gathered into the
+//     warp's arena when all its pages are resident;
 //   * otherwise the warp reads the list straight from host memory over the
 //     link (so every branch finishes where it started -- nothing is parked or
 //     lost, counts stay exact) and, for an absent page, claims a victim frame
@@ -52,10 +53,43 @@ __device__ __forceinline__ void ring_post(const DPaging& pg, unsigned long long 
   *(volatile unsigned long long*)&pg.ring_seq[slot & pg.ring_mask] = slot + 1;
 }
 
+// Frame state words: (page << 32) | pins.
+__device__ __forceinline__ int32_t fs_page(unsigned long long s) { return (int32_t)(s >> 32); }
+__device__ __forceinline__ uint32_t fs_pins(unsigned long long s) { return (uint32_t)s; }
+
+__device__ __forceinline__ unsigned long long ld_vol64(const unsigned long long* p) {
+  return *(const volatile unsigned long long*)p;
+}
+
+// Atomic add on a frame state with acquire (pin) or release (unpin)
+// semantics at GPU scope.
+__device__ __forceinline__ unsigned long long fs_add_acquire(unsigned long long* p, unsigned long long v) {
+  unsigned long long old;
+  asm volatile("atom.add.acquire.gpu.u64 %0, [%1], %2;" : "=l"(old) : "l"(p), "l"(v) : "memory");
+  return old;
+}
+__device__ __forceinline__ void fs_add_release(unsigned long long* p, unsigned long long v) {
+  asm volatile("red.add.release.gpu.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+// CAS with release semantics: what this thread wrote before (the new page's
+// LOADING entry) is visible to a reader that sees the new tag.
+__device__ __forceinline__ unsigned long long fs_cas_release(unsigned long long* p, unsigned long long cmp,
+                                                             unsigned long long v) {
+  unsigned long long old;
+  asm volatile("atom.cas.release.gpu.b64 %0, [%1], %2, %3;" : "=l"(old) : "l"(p), "l"(cmp), "l"(v) : "memory");
+  return old;
+}
+
 // One thread (lane 0 of a warp, or a lane for its own list).  Starts
 // loading page p if it is absent: reserve a ring slot,
 // claim the page, find a frame (never-used frames first, then a bounded
 // CLOCK sweep), post the request.  Never waits for the host.
+//
+// Eviction of page q from frame h: the entry page_frame[q] goes h ->
+// EVICTING, then the frame's state goes (q, 0 pins) -> (p, 0 pins) by CAS,
+// so a reader that pinned h first makes the CAS fail (the entry is put back);
+// a reader that pins afterwards sees tag p and backs off.  The frame is then
+// LOADING for p (page_frame[p] = LOADING) until the host publishes it.
 static __device__ void request_page(const DPaging& pg, int32_t p, PageCounters& pc) {
   if (pg.n_static >= pg.n_frames) return;  // no evictable frame to load into
   if (ld_vol(&pg.page_frame[p]) != PAGE_ABSENT) return;
@@ -65,22 +99,25 @@ static __device__ void request_page(const DPaging& pg, int32_t p, PageCounters& 
     ring_post(pg, slot, -1, -1);  // someone else is loading it
     return;
   }
+  const unsigned long long tag_p = (unsigned long long)(uint32_t)p << 32;
   int32_t f = -1;
   const unsigned long long k = atomicAdd(pg.next_free, 1ull);
   const int64_t n_dyn = pg.n_frames - pg.n_static;  // evictable frames
   if (k < (unsigned long long)pg.n_frames) {
+    // a never-used frame: no page entry names it, so no reader can pin it
     f = (int32_t)k;
+    atomicExch(&pg.frame_state[f], tag_p);
   } else if (n_dyn > 0) {
     const int sweep = (int)min((int64_t)4096, 2 * n_dyn + 8);  // bounded CLOCK sweep
     for (int t = 0; t < sweep && f < 0; t++) {
       const int32_t h = pg.n_static + (int32_t)(atomicAdd(pg.clock_hand, 1ull) % (unsigned long long)n_dyn);
       if (pg.frame_ref[h]) { pg.frame_ref[h] = 0; continue; }
-      if (ld_vol(&pg.frame_pin[h]) != 0) continue;
-      const int32_t q = ld_vol(&pg.frame_page[h]);
+      const unsigned long long st = ld_vol64(&pg.frame_state[h]);
+      if (fs_pins(st) != 0) continue;
+      const int32_t q = fs_page(st);
       if (q < 0) continue;
-      if (atomicCAS(&pg.page_frame[q], h, PAGE_EVICTING) != h) continue;
-      __threadfence();
-      if (ld_vol(&pg.frame_pin[h]) != 0) {  // a reader pinned it meanwhile
+      if (atomicCAS(&pg.page_frame[q], h, PAGE_EVICTING) != h) continue;  // loading, or moved
+      if (fs_cas_release(&pg.frame_state[h], st, tag_p) != st) {  // a reader pinned it meanwhile
         atomicExch(&pg.page_frame[q], h);
         continue;
       }
@@ -95,29 +132,31 @@ static __device__ void request_page(const DPaging& pg, int32_t p, PageCounters& 
     pc.dropped++;
     return;
   }
-  atomicExch(&pg.frame_page[f], p);
   ring_post(pg, slot, p, f);
   pc.requests++;
 }
 
 // Pins the frame holding page p if it is resident; returns the frame or -1.
 // A static frame is returned as is: its entry never changes during a run.
+// The pin is one acquire add on the frame's state word; the tag it returns
+// says whether the frame still holds p.  The entry is read once more after
+// the pin: the frame may have been given back to p for a new load in between
+// (then the entry reads LOADING until the host publishes it again).
 __device__ __forceinline__ int32_t try_pin(const DPaging& pg, int32_t p) {
   const int32_t f = ld_vol(&pg.page_frame[p]);
   if (f < 0) return -1;
   if (f < pg.n_static) return f;
-  atomicAdd(&pg.frame_pin[f], 1);
-  __threadfence();
-  if (ld_vol(&pg.page_frame[p]) != f) {
-    atomicSub(&pg.frame_pin[f], 1);
+  const unsigned long long st = fs_add_acquire(&pg.frame_state[f], 1ull);
+  if (fs_page(st) != p || ld_vol(&pg.page_frame[p]) != f) {
+    fs_add_release(&pg.frame_state[f], ~0ull);  // -1
     return -1;
   }
-  pg.frame_ref[f] = 1;
+  if (!pg.frame_ref[f]) pg.frame_ref[f] = 1;
   return f;
 }
 
 __device__ __forceinline__ void unpin_frame(const DPaging& pg, int32_t f) {
-  if (f >= pg.n_static) atomicSub(&pg.frame_pin[f], 1);
+  if (f >= pg.n_static) fs_add_release(&pg.frame_state[f], ~0ull);
 }
 
 // Frame of page p0 when pages p0..p1 all sit in consecutive static frames (a

@@ -43,11 +43,12 @@ def test_oracle_generators_equal_product_generators(seed):
     assert np.array_equal(pm.gen_labels(70000, 8, seed), orc.gen_labels(70000, 8, seed))
 
 
-@pytest.mark.parametrize("name", sorted(SAMPLES))
+# the R-MAT record's graph (3.6e9 adjacency entries) is regenerated on the
+# device by the bench that uses it, which checks its digest there
+@pytest.mark.parametrize("name", sorted(k for k, v in SAMPLES.items() if v["graph"]["kind"] == "chung_lu"))
 def test_sample_fixture_reproduces(name):
     rec = SAMPLES[name]
     gd = rec["graph"]
-    assert gd["kind"] == "chung_lu"
     rp, ci = orc.gen_chung_lu(gd["n"], gd["m"], gd["gamma"], gd["i0"], gd["max_w"], gd["seed"])
     assert _digest(rp, ci) == rec["graph_sha256"]
     hg = pm.gen_chung_lu(gd["n"], gd["m"], gamma=gd["gamma"], i0=gd["i0"], max_w=gd["max_w"], seed=gd["seed"])
