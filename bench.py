@@ -385,8 +385,12 @@ def run_ours(args, workload):
     subset = bool(sample and sample.get("extra_roots"))
     if sample is not None and args.sample_roots:
         # profiling a part of the sample: its roots' counts are still checked
+        # positions past the verified roots select extra (timed, unverified) roots
         keep = [int(x) for x in args.sample_roots.split(",")]
-        sample = dict(sample, roots=[sample["roots"][i] for i in keep], extra_roots=[])
+        nv = len(sample["roots"])
+        extra = sample.get("extra_roots") or []
+        sample = dict(sample, roots=[sample["roots"][i] for i in keep if i < nv],
+                      extra_roots=[extra[i - nv] for i in keep if i >= nv])
         sample["raw_count"] = sum(r["raw_count"] for r in sample["roots"])
         sample["count"] = sum(r["count"] for r in sample["roots"])
         subset = True
@@ -559,6 +563,11 @@ def run_ours(args, workload):
             "arenas": {"bytes": int(st["arena_bytes"]), "borrowed": int(st["borrowed_arenas"]),
                        "pool": int(st["arena_pool"])},
         }
+        if achieved > peak:
+            line["roofline"]["note"] = (
+                "algorithmic bytes charge each set operation its whole operand lists, as the reference's "
+                "merge scans them; this kernel reads one label's group of a label-grouped list and searches "
+                "a long operand rather than scanning it, so frac above 1 is that difference, not bandwidth")
         if w.get("paged"):
             info = graph.info()
             link = st["h2d_page_bytes"] + st["zero_copy_bytes"]
@@ -566,6 +575,8 @@ def run_ours(args, workload):
                 "pages": int(info["n_pages"]), "frames": int(info["n_frames"]),
                 "static_frames": int(info["n_static_frames"]), "page_bytes": w["paged"]["page_bytes"],
                 "page_hits_last_step": int(st["page_hits"]), "h2d_page_bytes_last_step": int(st["h2d_page_bytes"]),
+                "page_requests_last_step": int(st["page_requests"]), "page_dropped_last_step": int(st["page_dropped"]),
+                "evictions_last_step": int(st["evictions"]),
                 "zero_copy_bytes_last_step": int(st["zero_copy_bytes"]),
                 "achieved_gbs": link / (st["kernel_ms"] / 1000.0) / 1e9 if st["kernel_ms"] > 0 else 0.0,
                 "nominal_gbs": 64.0, "nominal": "PCIe Gen5 x16, one direction"}
@@ -673,7 +684,10 @@ def run_learned(args, workload):
         res[mode] = {"kernel_ms": statistics.median(times), "page_hits": stats["page_hits"],
                      "page_misses": stats["page_misses"], "pages_loaded": stats["pages_loaded"],
                      "zero_copy_bytes": stats["zero_copy_bytes"], "h2d_page_bytes": stats["h2d_page_bytes"],
-                     "prefetch_requests": stats["prefetch_requests"], "splits": stats["splits"]}
+                     "prefetch_requests": stats["prefetch_requests"], "page_requests": stats["page_requests"],
+                     "page_dropped": stats["page_dropped"], "evictions": stats["evictions"],
+                     "phase_cycles": {k: int(stats[k]) for k in ("leaf_cycles", "level_cycles", "prefix_cycles")},
+                     "splits": stats["splits"]}
     line = {"metric": "query_ms_learned_vs_plain", "workload": workload, "count": count,
             "arms": res, "speedup": res["plain"]["kernel_ms"] / res["learned"]["kernel_ms"],
             "plain": "cold frame pool, CLOCK, reference root order",

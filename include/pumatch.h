@@ -331,6 +331,9 @@ typedef struct {
   uint64_t prefix_cycles;   /* ... recomputing the path prefix of a donated
                                range (the cost of moving work between warps) */
   uint64_t prefetch_requests; /* pages posted from the prefetch lists          */
+  uint64_t page_requests;   /* paged mode: page loads posted to the host     */
+  uint64_t page_dropped;    /* paged mode: loads not posted (ring full, or
+                               every evictable frame pinned or referenced)  */
 } pm_stats;
 
 /* Replaces the `_parallel_match` launch and the host reduction of per-warp

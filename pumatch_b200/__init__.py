@@ -79,7 +79,8 @@ class Stats(C.Structure):
                 ("arena_bytes", C.c_uint64), ("device_status", C.c_uint32), ("pad_", C.c_uint32),
                 ("warp_ns", C.c_uint64), ("idle_ns", C.c_uint64), ("borrowed_arenas", C.c_uint64),
                 ("arena_pool", C.c_uint64), ("leaf_cycles", C.c_uint64), ("level_cycles", C.c_uint64),
-                ("prefix_cycles", C.c_uint64), ("prefetch_requests", C.c_uint64)]
+                ("prefix_cycles", C.c_uint64), ("prefetch_requests", C.c_uint64),
+                ("page_requests", C.c_uint64), ("page_dropped", C.c_uint64)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_ if not k.endswith("_")}

@@ -2503,6 +2503,8 @@ static pm_status finish_launch(const Launch& L, const unsigned long long* host_c
     so.level_cycles = stt[ST_LEVEL_CYC];
     so.prefix_cycles = stt[ST_PREFIX_CYC];
     so.prefetch_requests = stt[ST_PREFETCH];
+    so.page_requests = stt[ST_REQUESTS];
+    so.page_dropped = stt[ST_DROPPED];
     so.arena_pool = (uint64_t)L.n_big;
     so.device_status = status;
   }
