@@ -248,8 +248,12 @@ typedef struct {
                                takes root chunks k, k+count, ...            */
   int32_t use_graph;        /* 1: capture the launch in a CUDA graph         */
   int32_t timeout_ms;       /* bound on every device wait; 0 = default       */
-  int64_t root_begin;       /* restrict to roots [root_begin, root_end) of
-                               the reference-ordered root list; -1 = all     */
+  int64_t root_begin;       /* restrict to positions [root_begin, root_end)
+                               of the reference-ordered root list, or of
+                               root_order when one is given; -1 = all.
+                               Per-root outputs and root_split are indexed
+                               by root id (the position in the reference
+                               order), whatever the range               */
   int64_t root_end;
   int32_t cold_cache;       /* paged mode: empty the frame pool before the run */
   int32_t high_occupancy;   /* kernel variant by register cap: 0 default (85

@@ -825,6 +825,18 @@ __device__ __forceinline__ unsigned leaf_walk(const MatchArgs& a, const WarpStat
     const int stop = min(tend, S.lexcl[j + 1]);
     const int32_t* src = a.colidx + S.lrb[j] + (unsigned long long)(t - jbeg);
     const int n = stop - t;
+    if (n < 8) {
+      // a short segment (light subtrees): all its loads issued at once
+      int v[7];
+#pragma unroll
+      for (int u = 0; u < 7; u++) v[u] = u < n ? __ldg(src + u) : 0;
+#pragma unroll
+      for (int u = 0; u < 7; u++)
+        if (u < n) test(v[u]);
+      t = stop;
+      j++;
+      continue;
+    }
     // scalar up to a 16-byte boundary, then 128-bit loads, two in flight
     int q = min(n, (int)((4 - ((reinterpret_cast<uintptr_t>(src) >> 2) & 3)) & 3));
     for (int u = 0; u < q; u++) test(__ldg(src + u));
@@ -1541,7 +1553,9 @@ __global__ void __launch_bounds__(MINB == 1 ? 512 : 256, MINB) match_kernel(cons
     const long long re = min((long long)P.nroots, rb + a.chunk);
     unsigned long long local = 0;
     for (long long r = rb; r < re && !w.err; r++) {
-      const long long rid = a.root_order ? (long long)a.root_order[r] : r;
+      // position r of the range; with an order, the order's entry there
+      const long long pos = P.rbase + r;
+      const long long rid = a.root_order ? (long long)a.root_order[pos] : pos;
       const int2 e = P.roots[rid];
       const unsigned long long b0 = w.bytes, r0 = w.reads;
       if (lane == 0) {
@@ -2307,9 +2321,10 @@ static pm_status setup_launch(pm_ctx* c, const pm_graph* g, const pm_plan* const
     if (o.root_begin >= 0) b = std::min<int64_t>(o.root_begin, e);
     if (o.root_end >= 0) e = std::min<int64_t>(o.root_end, e);
     if (e < b) e = b;
-    L->dp[i].roots = *roots + off + b;
+    L->dp[i].roots = *roots + off;
     off += (size_t)L->dp[i].nroots;
     L->dp[i].nroots = e - b;
+    L->dp[i].rbase = b;
   }
   // Candidate storage.  worst_* hold every materialised slot at its largest
   // possible size (and, paged, two gathered max-degree lists); each warp's own

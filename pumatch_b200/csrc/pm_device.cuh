@@ -39,8 +39,9 @@ struct DPlan {
   // plan does not have that shape
   int8_t l2_x, l2_y;
   int8_t pad_[6];
-  const int2* roots;              // (v0, v1) root edges, reference order
-  int64_t nroots;
+  const int2* roots;              // (v0, v1) root edges, reference order (the whole list)
+  int64_t nroots;                 // positions this launch processes
+  int64_t rbase;                  // first position: root_begin (0 = all)
 };
 
 // Page cache of the adjacency array (paged residency).  A page is a fixed

@@ -66,6 +66,10 @@ class CostModel:
         self.device = device
         self.mu = np.zeros(NIN, dtype=np.float32)
         self.sd = np.ones(NIN, dtype=np.float32)
+        # targets are fitted standardised (log costs sit near 15 while the
+        # output layer starts near 0), and predictions scaled back
+        self.tmu = np.zeros(NOUT, dtype=np.float32)
+        self.tsd = np.ones(NOUT, dtype=np.float32)
 
     def close(self):
         if self._h:
@@ -113,6 +117,11 @@ class CostModel:
         self.mu = xs.mean(0).float().cpu().numpy()
         self.sd = (xs.std(0).float().clamp_min(1e-3)).cpu().numpy()
         xn = self.normalise(x)
+        ts = t.double()
+        self.tmu = ts.mean(0).float().cpu().numpy()
+        self.tsd = (ts.std(0).float().clamp_min(1e-3)).cpu().numpy()
+        t = ((t - torch.as_tensor(self.tmu, device=t.device)) / torch.as_tensor(self.tsd, device=t.device))
+        t = t.float().contiguous()
         gen = torch.Generator(device="cpu").manual_seed(seed)
         hist = []
         n = xn.shape[0]
@@ -132,7 +141,9 @@ class CostModel:
         return hist
 
     def predict(self, x):
-        return self.forward_raw(self.normalise(x))
+        import torch
+        y = self.forward_raw(self.normalise(x))
+        return y * torch.as_tensor(self.tsd, device=y.device) + torch.as_tensor(self.tmu, device=y.device)
 
 
 def heavy_first_order(pred):

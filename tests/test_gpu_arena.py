@@ -74,10 +74,12 @@ def test_tiny_own_arenas_borrow_and_keep_counts(ctx, name, labeled, text, paged)
 def test_hub_lists_beyond_the_own_gather_space(ctx):
     """Paged lists longer than a warp's own gather half (16,384 words) are
     gathered into a borrowed arena."""
-    hg = pm.gen_chung_lu(200_000, 1_500_000, gamma=2.1, i0=10.0, max_w=40_000.0, seed=21)
+    hg = pm.gen_chung_lu(200_000, 2_000_000, gamma=2.0, i0=10.0, max_w=60_000.0, seed=21)
     assert hg.max_degree > 20_000
-    hg = pm.HostGraph(hg.rowptr, hg.colidx, pm.gen_labels(hg.n, 2, seed=22))
-    cases = [(False, P.to_g(*P.clique(4)), 0, 3000), (True, P.to_g(*P.cycle(4), [0, 1, 0, 1]), 0, 400)]
+    # one label: a labeled slot's label group is the whole list, so the hub's
+    # group exceeds the gather half too
+    hg = pm.HostGraph(hg.rowptr, hg.colidx, pm.gen_labels(hg.n, 1, seed=22))
+    cases = [(False, P.to_g(*P.clique(4)), 0, 3000), (True, P.to_g(*P.cycle(4), [0, 0, 0, 0]), 0, 150)]
     for labeled, text, b, e in cases:
         want, ost = _oracle(hg, text, labeled, b, e)
         g = pm.GraphPreprocessor.from_host(hg, labeled=labeled, paged=True, page_bytes=64 << 10,

@@ -175,6 +175,21 @@ def test_gpu_shards_and_root_ranges(ctx):
     a = ctx.match(g, [p], root_begin=0, root_end=cut)[0][0]
     b = ctx.match(g, [p], root_begin=cut, root_end=n)[0][0]
     assert a + b == total
+    # per-root counts are indexed by root id whatever the range, and a range
+    # with an order covers those positions of the order
+    full = torch.zeros(n, dtype=torch.int64, device="cuda")
+    ctx.match(g, [p], root_counts_ptr=full.data_ptr())
+    parts = torch.zeros(n, dtype=torch.int64, device="cuda")
+    ctx.match(g, [p], root_begin=0, root_end=cut, root_counts_ptr=parts.data_ptr())
+    ctx.match(g, [p], root_begin=cut, root_end=n, root_counts_ptr=parts.data_ptr())
+    assert torch.equal(parts, full)
+    order = torch.from_numpy(np.random.default_rng(5).permutation(n).astype(np.int32)).cuda()
+    byorder = torch.zeros(n, dtype=torch.int64, device="cuda")
+    got = [ctx.match(g, [p], root_order_ptr=order.data_ptr(), root_begin=lo, root_end=hi,
+                     root_counts_ptr=byorder.data_ptr())[0][0] for lo, hi in ((0, cut), (cut, 2 * cut), (2 * cut, n))]
+    assert sum(got) == total and torch.equal(byorder, full)
+    first = order[:cut].long()
+    assert got[0] == int(full[first].sum()) * p.PatternMultiplicity
 
 
 def small_graph(edges, n):
