@@ -402,7 +402,8 @@ def run_ours(args, workload):
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")  # > 126 MB L2
     shard = dict(shard_rank=rank, shard_count=world) if world > 1 else {}
     run_kw = dict(timeout_ms=args.timeout_s * 1000, high_occupancy=args.high_occupancy,
-                  leaf_per_lane=int(args.leaf_per_lane), lane_subtree_max=args.lane_subtree_max, **shard)
+                  leaf_per_lane=int(args.leaf_per_lane), lane_subtree_max=args.lane_subtree_max,
+                  host_page_copy=int(args.host_page_copy), **shard)
     if args.root_limit > 0:
         run_kw.update(root_begin=args.root_begin, root_end=args.root_begin + args.root_limit)
     # per-root counts of plan 0, for the parity check
@@ -577,6 +578,9 @@ def run_ours(args, workload):
                 "page_hits_last_step": int(st["page_hits"]), "h2d_page_bytes_last_step": int(st["h2d_page_bytes"]),
                 "page_requests_last_step": int(st["page_requests"]), "page_dropped_last_step": int(st["page_dropped"]),
                 "evictions_last_step": int(st["evictions"]),
+                "device_page_loads_last_step": int(st["device_page_loads"]),
+                "page_loads": "host service thread only" if args.host_page_copy else
+                              "warps copy pages of one-page lists; the rest through the host service thread",
                 "zero_copy_bytes_last_step": int(st["zero_copy_bytes"]),
                 "achieved_gbs": link / (st["kernel_ms"] / 1000.0) / 1e9 if st["kernel_ms"] > 0 else 0.0,
                 "nominal_gbs": 64.0, "nominal": "PCIe Gen5 x16, one direction"}
@@ -686,6 +690,7 @@ def run_learned(args, workload):
                      "zero_copy_bytes": stats["zero_copy_bytes"], "h2d_page_bytes": stats["h2d_page_bytes"],
                      "prefetch_requests": stats["prefetch_requests"], "page_requests": stats["page_requests"],
                      "page_dropped": stats["page_dropped"], "evictions": stats["evictions"],
+                     "device_page_loads": stats["device_page_loads"],
                      "phase_cycles": {k: int(stats[k]) for k in ("leaf_cycles", "level_cycles", "prefix_cycles")},
                      "splits": stats["splits"]}
     line = {"metric": "query_ms_learned_vs_plain", "workload": workload, "count": count,
@@ -811,6 +816,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--high-occupancy", type=int, default=0,
                     help="kernel variant: 0 default, 1 capped at 64 registers, 2 capped at 85, 3 uncapped")
+    ap.add_argument("--host-page-copy", action="store_true",
+                    help="paged: every page load through the host service thread (no warp-side copies)")
     ap.add_argument("--leaf-per-lane", type=int, default=0,
                     help="last level: 0 work-balanced in lane-contiguous parts (default), 1 one candidate per "
                          "lane, 2 work-balanced strided")

@@ -300,6 +300,10 @@ typedef struct {
                                 candidates a warp hands to idle warps (the
                                 split_level1 of that root; learned: lower
                                 for roots predicted heavy)                   */
+  int32_t host_page_copy;   /* paged mode: 1 = every page load goes through
+                               the host service thread; 0 (default) = a
+                               warp that misses on a list within one page
+                               copies the page into its frame itself       */
 } pm_run_opts;
 
 void pm_run_opts_default(pm_run_opts* o);
@@ -338,6 +342,8 @@ typedef struct {
   uint64_t page_requests;   /* paged mode: page loads posted to the host     */
   uint64_t page_dropped;    /* paged mode: loads not posted (ring full, or
                                every evictable frame pinned or referenced)  */
+  uint64_t device_page_loads; /* paged mode: pages a warp copied into a frame
+                               itself (included in pages_loaded)            */
 } pm_stats;
 
 /* Replaces the `_parallel_match` launch and the host reduction of per-warp

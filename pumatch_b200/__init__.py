@@ -67,7 +67,8 @@ class RunOpts(C.Structure):
                 ("root_counts", C.c_void_p), ("root_cost", C.c_void_p), ("root_order", C.c_void_p),
                 ("root_reads", C.c_void_p), ("own_arena_words", C.c_int64), ("max_borrowed", C.c_int32),
                 ("prefetch_ahead", C.c_int32), ("prefetch_off", C.c_void_p), ("prefetch_pages", C.c_void_p),
-                ("prefetch_chunks", C.c_int64), ("root_split", C.c_void_p)]
+                ("prefetch_chunks", C.c_int64), ("root_split", C.c_void_p),
+                ("host_page_copy", C.c_int32)]
 
 
 class Stats(C.Structure):
@@ -80,7 +81,8 @@ class Stats(C.Structure):
                 ("warp_ns", C.c_uint64), ("idle_ns", C.c_uint64), ("borrowed_arenas", C.c_uint64),
                 ("arena_pool", C.c_uint64), ("leaf_cycles", C.c_uint64), ("level_cycles", C.c_uint64),
                 ("prefix_cycles", C.c_uint64), ("prefetch_requests", C.c_uint64),
-                ("page_requests", C.c_uint64), ("page_dropped", C.c_uint64)]
+                ("page_requests", C.c_uint64), ("page_dropped", C.c_uint64),
+                ("device_page_loads", C.c_uint64)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_ if not k.endswith("_")}

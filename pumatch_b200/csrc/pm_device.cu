@@ -152,7 +152,8 @@ struct MatchArgs {
 
 enum { ST_SETOPS = 0, ST_BYTES = 1, ST_ROOTS = 2, ST_SPLITS = 3, ST_HITS = 4, ST_MISSES = 5,
        ST_ZC_BYTES = 6, ST_REQUESTS = 7, ST_EVICTIONS = 8, ST_DROPPED = 9, ST_WARP_NS = 10, ST_IDLE_NS = 11,
-       ST_BORROWS = 12, ST_LEAF_CYC = 13, ST_LEVEL_CYC = 14, ST_PREFIX_CYC = 15, ST_PREFETCH = 16 };
+       ST_BORROWS = 12, ST_LEAF_CYC = 13, ST_LEVEL_CYC = 14, ST_PREFIX_CYC = 15, ST_PREFETCH = 16,
+       ST_DEV_LOADS = 17, ST_DEV_BYTES = 18 };
 // control block words: cursors[32] counts[32] stats[kStatWords] status/active ...
 constexpr int kStatWords = 24;
 
@@ -1661,6 +1662,10 @@ __global__ void __launch_bounds__(MINB == 1 ? 512 : 256, MINB) match_kernel(cons
       atomicAdd(&a.stats[ST_REQUESTS], w.pc.requests);
       atomicAdd(&a.stats[ST_EVICTIONS], w.pc.evictions);
       atomicAdd(&a.stats[ST_DROPPED], w.pc.dropped);
+      if (w.pc.dev_loads) {
+        atomicAdd(&a.stats[ST_DEV_LOADS], w.pc.dev_loads);
+        atomicAdd(&a.stats[ST_DEV_BYTES], w.pc.dev_bytes);
+      }
     }
     if (w.err) atomicOr(a.status, w.err);
   }
@@ -2252,7 +2257,7 @@ extern "C" pm_status pm_debug_roots(pm_ctx* c, const pm_graph* g, const pm_plan*
 
 // One prepared persistent launch: plans, roots, geometry, kernel arguments.
 struct Launch {
-  bool labeled = false, paged = false, cold = false;
+  bool labeled = false, paged = false, cold = false, host_copy = false;
   int64_t n_big = 0;          // borrowed arenas
   size_t own_bytes = 0, big_bytes = 0;
   int nplans = 0;
@@ -2301,6 +2306,7 @@ static pm_status setup_launch(pm_ctx* c, const pm_graph* g, const pm_plan* const
   if (o.shard_rank < 0 || o.shard_rank >= shard_count) return fail(PM_ERR_INVALID, "bad shard_rank");
   L->paged = g->residency == PM_RESIDENT_PAGED;
   L->cold = o.cold_cache != 0;
+  L->host_copy = o.host_page_copy != 0;
 
   // root lists, concatenated
   size_t off = 0;
@@ -2463,6 +2469,7 @@ static pm_status setup_launch(pm_ctx* c, const pm_graph* g, const pm_plan* const
   if (L->paged) {
     st = paged_prepare(c, const_cast<pm_graph*>(g), L->cold, &a.pg);
     if (st != PM_OK) return st;
+    a.pg.dev_copy = L->host_copy ? 0 : 1;
   }
   return PM_OK;
 }
@@ -2520,6 +2527,9 @@ static pm_status finish_launch(const Launch& L, const unsigned long long* host_c
     so.prefetch_requests = stt[ST_PREFETCH];
     so.page_requests = stt[ST_REQUESTS];
     so.page_dropped = stt[ST_DROPPED];
+    so.device_page_loads = stt[ST_DEV_LOADS];
+    so.pages_loaded += stt[ST_DEV_LOADS];  // the service thread's count plus the warps'
+    so.h2d_page_bytes += stt[ST_DEV_BYTES];
     so.arena_pool = (uint64_t)L.n_big;
     so.device_status = status;
   }

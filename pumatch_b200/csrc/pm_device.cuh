@@ -66,7 +66,8 @@ struct DPaging {
   unsigned long long* ring_seq;    // mapped host: slot + 1 once written
   unsigned long long* host_tail;   // mapped host: slots the host consumed
   unsigned int ring_mask;
-  unsigned int pad1;
+  int32_t dev_copy;                // 1: a warp that misses on a one-page list copies the page itself
+  int64_t n_ints;                  // length of the paged host array (the last page may be short)
 };
 
 enum : int32_t { PAGE_ABSENT = -1, PAGE_LOADING = -2 };

@@ -259,6 +259,8 @@ pm_status paged_prepare(pm_ctx* c, pm_graph* g, bool cold, DPaging* out) {
   out->ring_seq = s->ring_seq_dev;
   out->host_tail = s->host_tail_dev;
   out->ring_mask = s->ring_slots - 1;
+  out->n_ints = g->nadj;
+  out->dev_copy = 1;
   return PM_OK;
 }
 

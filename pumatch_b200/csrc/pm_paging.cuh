@@ -18,7 +18,11 @@
 //     lost, counts stay exact) and, for an absent page, claims a victim frame
 //     with a bounded CLOCK sweep (skipping pinned and referenced frames) and
 //     posts (page, frame) to a ring in mapped host memory;
-//   * a host service thread copies posted pages into their frames with
+//   * a warp that misses on a list within one page copies that page into
+//     the claimed frame itself (16-byte loads from the mapped array) and
+//     publishes the entry after a fence; other loads (lane-level misses,
+//     lists over several pages, prefetch lists) are posted to a host service
+//     thread, which copies posted pages into their frames with
 //     cudaMemcpyAsync on a side stream and publishes each page by copying its
 //     page-table entry after the data (same stream, so the entry lands
 //     after the page).
@@ -31,7 +35,7 @@ namespace pm {
 enum : int32_t { PAGE_EVICTING = -3 };
 
 struct PageCounters {
-  unsigned long long hits, misses, zc_bytes, requests, evictions, dropped;
+  unsigned long long hits, misses, zc_bytes, requests, evictions, dropped, dev_loads, dev_bytes;
 };
 
 __device__ __forceinline__ int32_t ld_vol(const int32_t* p) { return *(const volatile int32_t*)p; }
@@ -80,25 +84,18 @@ __device__ __forceinline__ unsigned long long fs_cas_release(unsigned long long*
   return old;
 }
 
-// One thread (lane 0 of a warp, or a lane for its own list).  Starts
-// loading page p if it is absent: reserve a ring slot,
-// claim the page, find a frame (never-used frames first, then a bounded
-// CLOCK sweep), post the request.  Never waits for the host.
+// One thread.  Claims a frame for page p if p is absent: the entry goes
+// ABSENT -> LOADING, and a never-used frame or a CLOCK victim is tagged p.
+// Returns the frame, or -1 when p is not absent or no frame is free (then
+// the entry is ABSENT again).  The caller fills the frame and publishes it.
 //
 // Eviction of page q from frame h: the entry page_frame[q] goes h ->
 // EVICTING, then the frame's state goes (q, 0 pins) -> (p, 0 pins) by CAS,
 // so a reader that pinned h first makes the CAS fail (the entry is put back);
 // a reader that pins afterwards sees tag p and backs off.  The frame is then
-// LOADING for p (page_frame[p] = LOADING) until the host publishes it.
-static __device__ void request_page(const DPaging& pg, int32_t p, PageCounters& pc) {
-  if (pg.n_static >= pg.n_frames) return;  // no evictable frame to load into
-  if (ld_vol(&pg.page_frame[p]) != PAGE_ABSENT) return;
-  const unsigned long long slot = ring_reserve(pg);
-  if (slot == ~0ull) { pc.dropped++; return; }
-  if (atomicCAS(&pg.page_frame[p], PAGE_ABSENT, PAGE_LOADING) != PAGE_ABSENT) {
-    ring_post(pg, slot, -1, -1);  // someone else is loading it
-    return;
-  }
+// LOADING for p (page_frame[p] = LOADING) until it is published.
+static __device__ int32_t claim_frame(const DPaging& pg, int32_t p, PageCounters& pc) {
+  if (atomicCAS(&pg.page_frame[p], PAGE_ABSENT, PAGE_LOADING) != PAGE_ABSENT) return -1;  // someone else has it
   const unsigned long long tag_p = (unsigned long long)(uint32_t)p << 32;
   int32_t f = -1;
   const unsigned long long k = atomicAdd(pg.next_free, 1ull);
@@ -128,12 +125,71 @@ static __device__ void request_page(const DPaging& pg, int32_t p, PageCounters& 
   }
   if (f < 0) {  // every frame busy: stay on the host-read path
     atomicExch(&pg.page_frame[p], PAGE_ABSENT);
-    ring_post(pg, slot, -1, -1);
     pc.dropped++;
+  }
+  return f;
+}
+
+// One thread (lane 0 of a warp, or a lane for its own list).  Starts
+// loading page p if it is absent: reserve a ring slot, claim a frame, post
+// (page, frame) for the host service thread.  Never waits for the host.
+static __device__ void request_page(const DPaging& pg, int32_t p, PageCounters& pc) {
+  if (pg.n_static >= pg.n_frames) return;  // no evictable frame to load into
+  if (ld_vol(&pg.page_frame[p]) != PAGE_ABSENT) return;
+  const unsigned long long slot = ring_reserve(pg);
+  if (slot == ~0ull) { pc.dropped++; return; }
+  const int32_t f = claim_frame(pg, p, pc);
+  if (f < 0) {
+    ring_post(pg, slot, -1, -1);
     return;
   }
   ring_post(pg, slot, p, f);
   pc.requests++;
+}
+
+// Whole warp, p uniform.  Loads absent page p into a frame itself: claim a
+// frame, copy the page from the mapped host array (16-byte loads, eight in
+// flight per lane: 4 KB per round trip for the warp), then publish the
+// entry after a fence.  Returns the frame, or -1 (p not absent, or no frame).
+// The copy is bounded work; nothing waits on the host or on other warps.
+static __device__ int32_t warp_load_page(const DPaging& pg, int32_t p, PageCounters& pc) {
+  const int lane = threadIdx.x & 31;
+  int32_t f = -1;
+  if (lane == 0 && pg.n_static < pg.n_frames && ld_vol(&pg.page_frame[p]) == PAGE_ABSENT) f = claim_frame(pg, p, pc);
+  f = __shfl_sync(0xffffffffu, f, 0);
+  if (f < 0) return -1;
+  const int sh = pg.page_shift;
+  const int64_t first = (int64_t)p << sh;
+  const int n = (int)min((int64_t)1 << sh, pg.n_ints - first);
+  const int32_t* hsrc = pg.host_colidx + first;  // 16-byte aligned: pages start at multiples of 1,024 ints
+  int32_t* fdst = pg.frames + ((uint64_t)f << sh);
+  const int4* src = reinterpret_cast<const int4*>(hsrc);
+  int4* dst = reinterpret_cast<int4*>(fdst);
+  const int nv = n >> 2;
+  for (int base = 0; base < nv; base += 256) {
+    int4 v[8];
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+      const int i = base + q * 32 + lane;
+      v[q] = i < nv ? src[i] : make_int4(0, 0, 0, 0);
+    }
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+      const int i = base + q * 32 + lane;
+      if (i < nv) __stcg(dst + i, v[q]);
+    }
+  }
+  for (int i = 4 * nv + lane; i < n; i += 32) __stcg(fdst + i, hsrc[i]);
+  __threadfence();  // each lane's stores before the publish below
+  __syncwarp();
+  if (lane == 0) {
+    pg.frame_ref[f] = 1;  // not the first victim of the next sweep
+    atomicExch(&pg.page_frame[p], f);
+    pc.dev_loads++;
+    pc.dev_bytes += 4ull * (unsigned long long)n;
+  }
+  __syncwarp();
+  return f;
 }
 
 // Pins the frame holding page p if it is resident; returns the frame or -1.
@@ -216,10 +272,12 @@ static __device__ ListRef paged_list(const DPaging& pg, uint64_t b, int len, int
   const int32_t p1 = (int32_t)((b + (uint64_t)len - 1) >> sh);
   int mode = 1;  // 0 frame, 1 host read, 2 gathered
   int32_t f0 = -1;
+  int32_t load = -1;  // a one-page list on an absent page: the warp loads the page
   if (lane == 0) {
     if (p0 == p1) {
       f0 = try_pin(pg, p0);
       if (f0 >= 0) mode = 0;
+      else if (pg.dev_copy && pg.n_static < pg.n_frames && ld_vol(&pg.page_frame[p0]) == PAGE_ABSENT) load = p0;
       else request_page(pg, p0, pc);
     } else if ((f0 = static_run(pg, p0, p1)) >= 0) {
       mode = 0;  // contiguous in the static frames: read in place, no pins
@@ -238,16 +296,25 @@ static __device__ ListRef paged_list(const DPaging& pg, uint64_t b, int len, int
           if (ld_vol(&pg.page_frame[j]) == PAGE_ABSENT) { request_page(pg, j, pc); posted++; }
       }
     }
-    if (mode == 1) { pc.misses++; pc.zc_bytes += 4ull * (unsigned long long)len; }
+    if (mode == 1) pc.misses++;
     else pc.hits++;
   }
   mode = __shfl_sync(0xffffffffu, mode, 0);
   f0 = __shfl_sync(0xffffffffu, f0, 0);
+  load = __shfl_sync(0xffffffffu, load, 0);
+  if (load >= 0 && warp_load_page(pg, load, pc) >= 0) {
+    if (lane == 0) f0 = try_pin(pg, load);  // fails only if evicted at once
+    f0 = __shfl_sync(0xffffffffu, f0, 0);
+    if (f0 >= 0) mode = 0;
+  }
   if (mode == 0) {
     const uint64_t off = b & ((1ull << sh) - 1);
     return ListRef{pg.frames + ((uint64_t)f0 << sh) + off, len, f0, f0 >= pg.n_static};
   }
-  if (mode == 1) return host_list_copy(pg.host_colidx + b, len, gather);
+  if (mode == 1) {
+    if (lane == 0) pc.zc_bytes += 4ull * (unsigned long long)len;
+    return host_list_copy(pg.host_colidx + b, len, gather);
+  }
   // gather the pinned pages into the arena, then unpin them
   __syncwarp();
   const uint64_t e = b + (uint64_t)len;

@@ -155,7 +155,8 @@ int main(void){
  printf("%zu %zu %zu %zu %zu %zu\n", offsetof(pm_run_opts, prefetch_ahead), offsetof(pm_run_opts, prefetch_off),
         offsetof(pm_run_opts, prefetch_pages), offsetof(pm_run_opts, prefetch_chunks), offsetof(pm_stats, prefetch_requests),
         offsetof(pm_run_opts, root_split));
- printf("%zu %zu\n", offsetof(pm_stats, page_requests), offsetof(pm_stats, page_dropped));
+ printf("%zu %zu %zu %zu\n", offsetof(pm_stats, page_requests), offsetof(pm_stats, page_dropped),
+        offsetof(pm_stats, device_page_loads), offsetof(pm_run_opts, host_page_copy));
  return 0; }'''
     import ctypes as C
     import tempfile
@@ -172,7 +173,8 @@ int main(void){
                     pm.Stats.prefix_cycles.offset, pm.RunOpts.prefetch_ahead.offset, pm.RunOpts.prefetch_off.offset,
                     pm.RunOpts.prefetch_pages.offset, pm.RunOpts.prefetch_chunks.offset,
                     pm.Stats.prefetch_requests.offset, pm.RunOpts.root_split.offset,
-                    pm.Stats.page_requests.offset, pm.Stats.page_dropped.offset]
+                    pm.Stats.page_requests.offset, pm.Stats.page_dropped.offset,
+                    pm.Stats.device_page_loads.offset, pm.RunOpts.host_page_copy.offset]
 
 
 def test_c_program_links_and_runs_host_entry_points(tmp_path):

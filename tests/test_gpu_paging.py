@@ -97,16 +97,44 @@ def test_paged_static_frames_exact(ctx, page_kb, frames, static):
         g.close()
 
 
-def test_paged_pressure_evicts_and_loads(ctx):
+@pytest.mark.parametrize("host_copy", [0, 1], ids=["warp-copies", "host-copies"])
+def test_paged_pressure_evicts_and_loads(ctx, host_copy):
+    """Under eviction pressure, with pages loaded by the missing warps
+    themselves (default) or all through the host service thread."""
     hg = workload()
     g = pm.GraphPreprocessor.from_host(hg, labeled=True, paged=True, page_bytes=4096, frame_pool_bytes=32 * 4096)
     text, _ = TEXTS["C5_lab"]
     want, _ = oracle(hg, "C5_lab")
-    got, st = ctx.match(g, [pm.PatternPreprocessor(text=text, labeled=True)], cold_cache=True)
+    got, st = ctx.match(g, [pm.PatternPreprocessor(text=text, labeled=True)], cold_cache=True,
+                        host_page_copy=host_copy)
     assert got[0] == want
     assert st["pages_loaded"] > 0 and st["evictions"] > 0
-    assert st["h2d_page_bytes"] == st["pages_loaded"] * 4096 or st["h2d_page_bytes"] <= st["pages_loaded"] * 4096
+    assert st["h2d_page_bytes"] <= st["pages_loaded"] * 4096
     assert st["page_hits"] + st["page_misses"] > 0
+    if host_copy:
+        assert st["device_page_loads"] == 0
+    else:
+        assert st["device_page_loads"] > 0
+    g.close()
+
+
+@pytest.mark.parametrize("page_kb,frames", [(4, 16), (64, 4), (16, 8)])
+def test_paged_host_copies_exact(ctx, page_kb, frames):
+    """Every page load through the host service thread: the same counts."""
+    hg = workload()
+    pb = page_kb << 10
+    for labeled in (True, False):
+        g = pm.GraphPreprocessor.from_host(hg, labeled=labeled, paged=True, page_bytes=pb,
+                                           frame_pool_bytes=frames * pb)
+        for name, (text, lab) in TEXTS.items():
+            if lab != labeled:
+                continue
+            want, ost = oracle(hg, name)
+            got, st = ctx.match(g, [pm.PatternPreprocessor(text=text, labeled=labeled)], cold_cache=True,
+                                host_page_copy=1, timeout_ms=120000)
+            assert got[0] == want and st["set_ops"] == ost["set_ops"], (name, page_kb, frames)
+            assert st["device_page_loads"] == 0
+        g.close()
 
 
 def test_paged_full_pool_matches_hbm(ctx):
