@@ -826,18 +826,6 @@ __device__ __forceinline__ unsigned leaf_walk(const MatchArgs& a, const WarpStat
     const int stop = min(tend, S.lexcl[j + 1]);
     const int32_t* src = a.colidx + S.lrb[j] + (unsigned long long)(t - jbeg);
     const int n = stop - t;
-    if (n < 8) {
-      // a short segment (light subtrees): all its loads issued at once
-      int v[7];
-#pragma unroll
-      for (int u = 0; u < 7; u++) v[u] = u < n ? __ldg(src + u) : 0;
-#pragma unroll
-      for (int u = 0; u < 7; u++)
-        if (u < n) test(v[u]);
-      t = stop;
-      j++;
-      continue;
-    }
     // scalar up to a 16-byte boundary, then 128-bit loads, two in flight
     int q = min(n, (int)((4 - ((reinterpret_cast<uintptr_t>(src) >> 2) & 3)) & 3));
     for (int u = 0; u < q; u++) test(__ldg(src + u));
@@ -1009,6 +997,7 @@ __device__ unsigned long long leaf_batch(const MatchArgs& a, const DPlan& P, War
     const bool mine = i < e;
     const int c = mine ? cand[i] : 0;
     bool deferred = false;
+    int32_t want = -1;  // an absent page this lane read around, for the warp to load
     if (mine) {
       const int ub = self_ub ? min(common_ub, c) : common_ub;
       if (kind == SLOT_COPY) {  // unlabeled: A = parent slot minus the candidate
@@ -1051,8 +1040,12 @@ __device__ unsigned long long leaf_batch(const MatchArgs& a, const DPlan& P, War
             } else if (p0 == p1 && gr.y <= PM_LANE_MAX) {
               // a short list on a missing page: this lane copies it from host
               // memory into its own part of the gather space, 16 reads in
-              // flight per round trip, and asks for the page
-              if (ld_vol(&a.pg.page_frame[p0]) == PAGE_ABSENT) request_page(a.pg, p0, lpc);
+              // flight per round trip, and notes the page for the warp to
+              // load after the batch (or posts it to the host thread)
+              if (ld_vol(&a.pg.page_frame[p0]) == PAGE_ABSENT) {
+                if (a.pg.dev_copy) want = p0;
+                else request_page(a.pg, p0, lpc);
+              }
               const int32_t* src = a.pg.host_colidx + s0;
               int32_t* stage = S.gather + lane * PM_LANE_MAX;
               for (int x = 0; x < gr.y; x += 16) {
@@ -1171,6 +1164,16 @@ __device__ unsigned long long leaf_batch(const MatchArgs& a, const DPlan& P, War
       if (lane == 0) S.path[Lf] = cc;
       __syncwarp();
       cnt_warp += (unsigned long long)run_slot<LABELED, PAGED>(a, P, S, Lf, s, S.top[Lf], true, w);
+    }
+    if (PAGED) {
+      // pages the lanes read around: the warp loads up to two of them per
+      // 32 candidates (one page copy each), so later reads hit
+      unsigned wm = __ballot_sync(FULL, want >= 0);
+      for (int k = 0; k < 2 && wm; k++) {
+        const int src = __ffs(wm) - 1;
+        wm &= wm - 1;
+        warp_load_page(a.pg, __shfl_sync(FULL, want, src), w.pc);
+      }
     }
   }
   if (PAGED) {

@@ -20,9 +20,11 @@
 //     posts (page, frame) to a ring in mapped host memory;
 //   * a warp that misses on a list within one page copies that page into
 //     the claimed frame itself (16-byte loads from the mapped array) and
-//     publishes the entry after a fence; other loads (lane-level misses,
-//     lists over several pages, prefetch lists) are posted to a host service
-//     thread, which copies posted pages into their frames with
+//     publishes the entry after a fence, and so does a warp for up to two
+//     pages its lanes missed on in a last-level batch; other loads (lists
+//     over several pages, prefetch lists, and every load when the run asks
+//     for host copies) are posted to a host service thread, which copies
+//     posted pages into their frames with
 //     cudaMemcpyAsync on a side stream and publishes each page by copying its
 //     page-table entry after the data (same stream, so the entry lands
 //     after the page).
@@ -152,7 +154,7 @@ static __device__ void request_page(const DPaging& pg, int32_t p, PageCounters& 
 // flight per lane: 4 KB per round trip for the warp), then publish the
 // entry after a fence.  Returns the frame, or -1 (p not absent, or no frame).
 // The copy is bounded work; nothing waits on the host or on other warps.
-static __device__ int32_t warp_load_page(const DPaging& pg, int32_t p, PageCounters& pc) {
+static __device__ __noinline__ int32_t warp_load_page(const DPaging& pg, int32_t p, PageCounters& pc) {
   const int lane = threadIdx.x & 31;
   int32_t f = -1;
   if (lane == 0 && pg.n_static < pg.n_frames && ld_vol(&pg.page_frame[p]) == PAGE_ABSENT) f = claim_frame(pg, p, pc);
@@ -263,49 +265,73 @@ __device__ __forceinline__ ListRef host_list_copy(const int32_t* src, int len, i
 // shared scratch of PM_MAX_LIST_PAGES frame indices.  Frames are remembered
 // from the pin, never re-read from the table (an evictor can hold an entry at
 // PAGE_EVICTING for a moment even while the frame is pinned).
-static __device__ ListRef paged_list(const DPaging& pg, uint64_t b, int len, int32_t* gather, int32_t* pins,
+static __device__ __noinline__ ListRef paged_list(const DPaging& pg, uint64_t b, int len, int32_t* gather, int32_t* pins,
                                      PageCounters& pc) {
   const int lane = threadIdx.x & 31;
   if (len == 0) return ListRef{pg.host_colidx + b, 0, -1};
   const int sh = pg.page_shift;
   const int32_t p0 = (int32_t)(b >> sh);
   const int32_t p1 = (int32_t)((b + (uint64_t)len - 1) >> sh);
-  int mode = 1;  // 0 frame, 1 host read, 2 gathered
+  const bool can_load = pg.dev_copy && pg.n_static < pg.n_frames;
+  int mode = 1;  // 0 frame, 1 host read, 2 gathered, 3 several pages to pin
   int32_t f0 = -1;
   int32_t load = -1;  // a one-page list on an absent page: the warp loads the page
   if (lane == 0) {
     if (p0 == p1) {
       f0 = try_pin(pg, p0);
       if (f0 >= 0) mode = 0;
-      else if (pg.dev_copy && pg.n_static < pg.n_frames && ld_vol(&pg.page_frame[p0]) == PAGE_ABSENT) load = p0;
+      else if (can_load && ld_vol(&pg.page_frame[p0]) == PAGE_ABSENT) load = p0;
       else request_page(pg, p0, pc);
     } else if ((f0 = static_run(pg, p0, p1)) >= 0) {
       mode = 0;  // contiguous in the static frames: read in place, no pins
     } else if (p1 - p0 < PM_MAX_LIST_PAGES) {
-      int32_t k = p0;
-      for (; k <= p1; k++) {
-        const int32_t f = try_pin(pg, k);
-        if (f < 0) break;
-        pins[k - p0] = f;
-      }
-      if (k > p1) {
-        mode = 2;
-      } else {
-        for (int32_t j = p0; j < k; j++) unpin_frame(pg, pins[j - p0]);
-        for (int32_t j = p0, posted = 0; j <= p1 && posted < 4; j++)
-          if (ld_vol(&pg.page_frame[j]) == PAGE_ABSENT) { request_page(pg, j, pc); posted++; }
-      }
+      mode = 3;
     }
-    if (mode == 1) pc.misses++;
-    else pc.hits++;
   }
   mode = __shfl_sync(0xffffffffu, mode, 0);
   f0 = __shfl_sync(0xffffffffu, f0, 0);
   load = __shfl_sync(0xffffffffu, load, 0);
+  bool hit = mode == 0;
   if (load >= 0 && warp_load_page(pg, load, pc) >= 0) {
     if (lane == 0) f0 = try_pin(pg, load);  // fails only if evicted at once
     f0 = __shfl_sync(0xffffffffu, f0, 0);
     if (f0 >= 0) mode = 0;
+  }
+  if (mode == 3) {
+    // several pages: the lanes pin them (page p0 + lane, p0 + lane + 32);
+    // when some are absent the warp loads them one by one and pins again
+    // (only when a quarter of the evictable frames holds them all; else a
+    // list's own loads would evict each other)
+    const bool load_all = can_load && 4ll * (p1 - p0 + 1) <= pg.n_frames - pg.n_static;
+    bool all = false;
+    for (int attempt = 0; attempt < 2 && !all; attempt++) {
+      if (attempt == 1) {
+        if (!load_all) {
+          if (lane == 0)
+            for (int32_t j = p0, posted = 0; j <= p1 && posted < 4; j++)
+              if (ld_vol(&pg.page_frame[j]) == PAGE_ABSENT) { request_page(pg, j, pc); posted++; }
+          break;
+        }
+        for (int32_t k = p0; k <= p1; k++) warp_load_page(pg, k, pc);
+      }
+      bool ok = true;
+      for (int32_t k = p0 + lane; k <= p1; k += 32) {
+        const int32_t f = try_pin(pg, k);
+        pins[k - p0] = f;
+        ok = ok && f >= 0;
+      }
+      all = __all_sync(0xffffffffu, ok);
+      if (!all)
+        for (int32_t k = p0 + lane; k <= p1; k += 32)
+          if (pins[k - p0] >= 0) unpin_frame(pg, pins[k - p0]);
+      if (attempt == 0) hit = all;
+    }
+    __syncwarp();
+    mode = all ? 2 : 1;
+  }
+  if (lane == 0) {
+    if (hit) pc.hits++;
+    else pc.misses++;
   }
   if (mode == 0) {
     const uint64_t off = b & ((1ull << sh) - 1);
@@ -316,7 +342,6 @@ static __device__ ListRef paged_list(const DPaging& pg, uint64_t b, int len, int
     return host_list_copy(pg.host_colidx + b, len, gather);
   }
   // gather the pinned pages into the arena, then unpin them
-  __syncwarp();
   const uint64_t e = b + (uint64_t)len;
   for (int32_t k = p0; k <= p1; k++) {
     const int32_t f = pins[k - p0];
@@ -326,8 +351,7 @@ static __device__ ListRef paged_list(const DPaging& pg, uint64_t b, int len, int
     for (uint64_t i = lane; i < s1 - s0; i += 32) dst[i] = __ldcg(src + i);
   }
   __syncwarp();
-  if (lane == 0)
-    for (int32_t k = p0; k <= p1; k++) unpin_frame(pg, pins[k - p0]);
+  for (int32_t k = p0 + lane; k <= p1; k += 32) unpin_frame(pg, pins[k - p0]);
   __syncwarp();
   return ListRef{gather, len, -1};
 }
