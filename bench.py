@@ -381,6 +381,9 @@ def run_ours(args, workload):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local))
     w, hg, texts = build_workload(workload)
+    if args.static_frac is not None and w.get("paged") and "frame_bytes" in w["paged"]:
+        # part of the absolute pool placed once and never evicted (the array's first pages)
+        w = dict(w, paged=dict(w["paged"], static_bytes=int(args.static_frac * w["paged"]["frame_bytes"])))
     sample = load_sample(w, hg, args.samples)
     subset = bool(sample and sample.get("extra_roots"))
     if sample is not None and args.sample_roots:
@@ -816,6 +819,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--high-occupancy", type=int, default=0,
                     help="kernel variant: 0 default, 1 capped at 64 registers, 2 capped at 85, 3 uncapped")
+    ap.add_argument("--static-frac", type=float, default=None,
+                    help="paged workloads with an absolute pool: this share of it static (never evicted)")
     ap.add_argument("--host-page-copy", action="store_true",
                     help="paged: every page load through the host service thread (no warp-side copies)")
     ap.add_argument("--leaf-per-lane", type=int, default=0,

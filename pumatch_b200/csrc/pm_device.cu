@@ -1537,7 +1537,13 @@ __global__ void __launch_bounds__(MINB == 1 ? 512 : 256, MINB) match_kernel(cons
     if (PAGED && a.pf_off && p == 0) {
       // post the predicted pages of a chunk this warp's successors will reach
       const long long pc = (long long)gc + (long long)a.pf_ahead * a.shard_count;
-      if (pc < a.pf_chunks) {
+      // only while the host's queue is short: a page posted behind a long
+      // queue stays LOADING, and warps that miss on it meanwhile can neither
+      // read it from a frame nor load it themselves
+      unsigned long long queued = 0;
+      if (lane == 0) queued = *(volatile unsigned long long*)a.pg.ring_head - *(volatile unsigned long long*)a.pg.host_tail;
+      queued = __shfl_sync(FULL, queued, 0);  // one decision for the warp (the block below shuffles)
+      if (pc < a.pf_chunks && queued < 64) {
         PageCounters lpc = {};
         for (int k = a.pf_off[pc] + lane; k < a.pf_off[pc + 1]; k += 32) {
           const int32_t pg = a.pf_pages[k];
