@@ -21,6 +21,14 @@ count read-back inside the timed region).  With N>1 ranks the root chunks are
 sharded across ranks (rank r takes chunks r, r+N, ...) and the counts are
 summed with one 8-byte all-reduce per pattern.
 
+The default line (one GPU) also carries the two comparisons the metric
+names, measured after the timed steps: `batched_vs_sequential` (twenty
+patterns in one persistent launch vs one launch each) and `learned_vs_plain`
+(learned residency, order, prefetch and split thresholds vs a cold CLOCK pool
+on a paged graph, with the model's prediction error beside a constant
+predictor's), both on R-MAT graphs of 2^17 vertices with identical counts
+across arms.  --no-comparisons leaves them out.
+
 --impl reference times the CPU implementation of the same path (the oracle
 port; the reference itself has no CPU implementation of its matcher) on all
 host cores, one bounded sample of the same roots per step, rank 0 only; it
@@ -601,6 +609,9 @@ def run_ours(args, workload):
                 parity = {"roots_checked": int(len(idx)), "ok": ok, "mismatched_roots": bad[:16],
                           "against": "oracle per-root counts on the CPU baseline's seeded root sample"}
         line["parity"] = parity
+        if (world == 1 and workload == DEFAULT_WORKLOAD and not args.no_comparisons and not args.sample_roots
+                and args.root_limit == 0):
+            line.update(comparisons(args))
         print(json.dumps(line), flush=True)
         if not ok:
             sys.exit(1)
@@ -611,7 +622,7 @@ def run_ours(args, workload):
         dist.destroy_process_group()
 
 
-def run_learned(args, workload):
+def learned_compare(args, workload):
     """Plain vs learned on the workload's paged graph, the model trained on
     plain runs over three other seeds of the same generator.
 
@@ -705,10 +716,13 @@ def run_learned(args, workload):
             "train_s": train_s, "train_roots": int(x.shape[0]), "eval_roots": int(xe.shape[0]),
             "frames": int(info["n_frames"]), "pages": int(info["n_pages"]),
             "prefetch_pages_listed": int(len(pf_pages))}
-    print(json.dumps(line), flush=True)
+    g.close()
+    model.close()
+    ctx.close()
+    return line
 
 
-def run_batch_compare(args, workload):
+def run_batch_compare(args, workload, emit=True):
     """One batched persistent launch (and its CUDA-graph replay) vs the same
     patterns launched one by one, over the same roots; optional autotuner
     sweep.  With --root-frac/--root-limit every pattern runs the root
@@ -756,6 +770,10 @@ def run_batch_compare(args, workload):
             "counts_equal": "batched, graph replay and sequential"}
     if w.get("paged"):
         line["paged"] = w["paged"]
+    if not emit:
+        g.close()
+        ctx.close()
+        return line
     print(json.dumps(line), flush=True)
     if args.autotune:
         from pumatch_b200 import autotune
@@ -770,6 +788,44 @@ def run_batch_compare(args, workload):
         print(json.dumps(tuned), flush=True)
     g.close()
     ctx.close()
+    return line
+
+
+def comparisons(args):
+    """The two comparisons the metric names, for the default line: the
+    20-pattern batch in one launch vs one launch per pattern, and learned vs
+    plain scheduling on a paged graph (stand-ins of the configured batch and
+    learned queries at 2^17 vertices; the standalone --compare-sequential and
+    --learned runs print the full records).  A failure is reported in the
+    line, not raised: the default line's own measurement stands."""
+    import copy
+    sub = copy.copy(args)
+    sub.steps, sub.warmup, sub.root_limit, sub.autotune = 2, 1, 0, False
+    out = {}
+    try:
+        b = run_batch_compare(sub, "rmat128k_batch20_lab32", emit=False)
+        out["batched_vs_sequential"] = {k: b[k] for k in ("workload", "batched_ms", "graph_replay_kernel_ms",
+                                                           "sequential_ms", "speedup")}
+        out["batched_vs_sequential"].update(patterns=len(b["patterns"]), counts_equal=True)
+    except Exception as e:  # noqa: BLE001 -- reported in the line
+        out["batched_vs_sequential"] = {"error": f"{type(e).__name__}: {e}"[:300]}
+    try:
+        sub.steps, sub.warmup = 3, 1
+        ln = learned_compare(sub, "rmat128k_c5t2_lab32_clock")
+        arms = ln["arms"]
+        out["learned_vs_plain"] = {
+            "workload": ln["workload"], "plain_ms": arms["plain"]["kernel_ms"],
+            "learned_residency_order_ms": arms["learned_residency_order"]["kernel_ms"],
+            "learned_ms": arms["learned"]["kernel_ms"],
+            "speedup_residency_order": arms["plain"]["kernel_ms"] / arms["learned_residency_order"]["kernel_ms"],
+            "speedup": ln["speedup"],
+            "page_misses": {k: v["page_misses"] for k, v in arms.items()},
+            "prediction_mae_log": ln["prediction_mae_log"],
+            "constant_predictor_mae_log": ln["constant_predictor_mae_log"],
+            "counts_equal": True, "plain": ln["plain"], "learned": ln["learned"]}
+    except Exception as e:  # noqa: BLE001
+        out["learned_vs_plain"] = {"error": f"{type(e).__name__}: {e}"[:300]}
+    return out
 
 
 def run_ref_gpu_table(args):
@@ -841,13 +897,15 @@ def main():
     ap.add_argument("--prefetch-pages", type=int, default=64, help="learned: pages listed per root chunk")
     ap.add_argument("--compare-sequential", action="store_true", help="batched vs one launch per pattern")
     ap.add_argument("--autotune", action="store_true", help="with --compare-sequential: sweep launch configs")
+    ap.add_argument("--no-comparisons", action="store_true",
+                    help="default line without the batched and learned comparisons")
     ap.add_argument("--ref-gpu-table", action="store_true",
                     help="this build's kernel ms beside the reference GPU binary's on its golden cases")
     args = ap.parse_args()
     if args.ref_gpu_table:
         run_ref_gpu_table(args)
     elif args.learned:
-        run_learned(args, args.workload)
+        print(json.dumps(learned_compare(args, args.workload)), flush=True)
     elif args.compare_sequential:
         run_batch_compare(args, args.workload)
     elif args.impl == "reference":
