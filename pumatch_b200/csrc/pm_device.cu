@@ -735,8 +735,8 @@ __device__ __forceinline__ bool in_table(const int32_t* t, int bits, int x) {
 // Membership structures for a leaf batch's common operand B (sorted), built
 // in the warp's shared staging buffer (PM_SB_MAX words):
 enum : int {
-  MEMB_BITMAP = 0,  // max B < 32 * PM_SB_MAX (and |B| > 32 or max B < 2048): one bit per id in [0, max B]
-  MEMB_FILTER = 1,  // 32 < |B| <= PM_SB_MAX / 4: a one-hash filter of 16 * PM_SB_MAX bits, then a hash table
+  MEMB_BITMAP = 0,  // max B < 32 * PM_SB_MAX: one bit per id in [0, max B]
+  MEMB_FILTER = 1,  // |B| <= PM_SB_MAX / 4: a one-hash filter of 16 * PM_SB_MAX bits, then a hash table
   MEMB_HASH = 2,    // |B| <= PM_SB_MAX / 2: an open-addressing table at most half full
   MEMB_SORTED = 3   // else: the sorted copy, binary search
 };
@@ -770,17 +770,14 @@ __device__ int leaf_build(WarpState& S, const int32_t* B, int lenB, LeafSet& m) 
   m.hi = lenB ? B[lenB - 1] : 0;
   m.bits = 5;
   int mode;
-  // a bitmap costs one cleared word per 32 ids of [0, max B]: for a few
-  // elements spread over a wide range a small hash table is cheaper to build
-  const int bm_words = (m.hi >> 5) + 1;
-  if (m.hi < 32 * PM_SB_MAX && (lenB > 32 || bm_words <= 64)) {
+  if (m.hi < 32 * PM_SB_MAX) {
     mode = MEMB_BITMAP;
     const int words = lenB ? (m.hi >> 5) + 1 : 0;
     for (int i = lane; i < words; i += 32) S.sb[i] = 0;
     __syncwarp();
     for (int i = lane; i < lenB; i += 32) atomicOr((unsigned int*)&S.sb[B[i] >> 5], 1u << (B[i] & 31));
   } else if (lenB <= PM_SB_MAX / 2) {
-    mode = (lenB <= PM_SB_MAX / 4 && lenB > 32) ? MEMB_FILTER : MEMB_HASH;
+    mode = lenB <= PM_SB_MAX / 4 ? MEMB_FILTER : MEMB_HASH;
     int32_t* tab = S.sb + (mode == MEMB_FILTER ? PM_SB_MAX / 2 : 0);
     const int cap = mode == MEMB_FILTER ? PM_SB_MAX / 2 : PM_SB_MAX;
     while ((1 << m.bits) < 2 * lenB) m.bits++;
