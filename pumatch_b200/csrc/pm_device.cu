@@ -826,12 +826,19 @@ __device__ __forceinline__ unsigned leaf_walk(const MatchArgs& a, const WarpStat
     const int stop = min(tend, S.lexcl[j + 1]);
     const int32_t* src = a.colidx + S.lrb[j] + (unsigned long long)(t - jbeg);
     const int n = stop - t;
-    // scalar up to a 16-byte boundary, then 128-bit loads, two in flight
+    // scalar up to a 16-byte boundary, then 128-bit loads, four in flight (two, one at the tail)
     int q = min(n, (int)((4 - ((reinterpret_cast<uintptr_t>(src) >> 2) & 3)) & 3));
     for (int u = 0; u < q; u++) test(__ldg(src + u));
     const int4* v = reinterpret_cast<const int4*>(src + q);
     const int nv = (n - q) >> 2;
     int i = 0;
+    for (; i + 4 <= nv; i += 4) {
+      const int4 a0 = __ldg(v + i), a1 = __ldg(v + i + 1), a2 = __ldg(v + i + 2), a3 = __ldg(v + i + 3);
+      test(a0.x); test(a0.y); test(a0.z); test(a0.w);
+      test(a1.x); test(a1.y); test(a1.z); test(a1.w);
+      test(a2.x); test(a2.y); test(a2.z); test(a2.w);
+      test(a3.x); test(a3.y); test(a3.z); test(a3.w);
+    }
     for (; i + 2 <= nv; i += 2) {
       const int4 a0 = __ldg(v + i), a1 = __ldg(v + i + 1);
       test(a0.x); test(a0.y); test(a0.z); test(a0.w);
@@ -853,7 +860,7 @@ __device__ __forceinline__ unsigned leaf_walk(const MatchArgs& a, const WarpStat
 // candidates (each cut at its symmetry-breaking bound) are laid end to end
 // and split into 32 contiguous parts, one per lane.  A lane finds the
 // candidate owning its part's start once and walks on through the following
-// lists, four loads in flight, testing each element against B's structure in
+// lists, four 128-bit loads in flight, testing each element against B's structure in
 // shared memory (leaf_build).  Counts only; no truncation.  Same set
 // operations, counts and accounting as lane_intersect per candidate.
 // Batches averaging under 16 elements per lane, and a.leaf_flat == 2, use
