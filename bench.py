@@ -27,7 +27,12 @@ patterns in one persistent launch vs one launch each) and `learned_vs_plain`
 (learned residency, order, prefetch and split thresholds vs a cold CLOCK pool
 on a paged graph, with the model's prediction error beside a constant
 predictor's), both on R-MAT graphs of 2^17 vertices with identical counts
-across arms.  --no-comparisons leaves them out.
+across arms.  Two more follow on the same graphs: `paging_ablation`, the
+reference's residency ablations (device partition plus package buffer,
+partition only, buffer only, UM only) as pool splits of the paged path,
+beside the graph in HBM; and `page_size_tuning`, the autotuner's page-size
+axis (16, 64, 256 KB) on the twenty-pattern batch, paged.
+--no-comparisons leaves all four out.
 
 --impl reference times the CPU implementation of the same path (the oracle
 port; the reference itself has no CPU implementation of its matcher) on all
@@ -793,6 +798,103 @@ def run_batch_compare(args, workload, emit=True):
     return line
 
 
+def paging_ablation(args, workload="rmat128k_c5t2_lab32_paged", root_share=16, um_timeout_ms=8000):
+    """The reference's residency ablations (plot/plot_fig11.sh:139-166) on one
+    paged workload, as pool splits of the same paged path: the device
+    partition plus the package buffer (the workload's split), the partition
+    only (the whole pool static), the buffer only (the whole pool
+    evictable), and UM only (a pool of one page: every list read over the
+    host link); the graph in HBM beside them.  Every arm starts cold and runs
+    the first 1/root_share of the root list; counts must be equal.  The UM arm
+    has a shorter device deadline: past it, it is reported as timed out."""
+    import torch
+    torch.cuda.set_device(0)
+    ctx = pm.Context(0)
+    w, hg, texts = build_workload(workload)
+    labeled = w["labeled"]
+    p = pm.PatternPreprocessor(text=texts[0][1], labeled=labeled)
+    pg = w["paged"]
+    pb = pg["page_bytes"]
+    pool = max(pb, int(hg.colidx.nbytes * pg["frame_fraction"]) // pb * pb)
+    static = int(hg.colidx.nbytes * pg.get("static_fraction", 0.0)) // pb * pb
+    arms = {"hbm": None,
+            "partition_and_buffer": (pool, static),
+            "partition_only": (static, static),
+            "buffer_only": (pool, 0),
+            "um_only": (pb, 0)}
+    rows, want, rng = {}, None, None
+    for name, split in arms.items():
+        if split is None:
+            g = pm.GraphPreprocessor.from_host(hg, labeled=labeled, device=0)
+        else:
+            g = pm.GraphPreprocessor.from_host(hg, labeled=labeled, device=0, paged=True, page_bytes=pb,
+                                               frame_pool_bytes=split[0], static_pool_bytes=split[1])
+        try:
+            if rng is None:
+                rng = (0, max(1, ctx.count_roots(g, p) // root_share))
+            kw = dict(root_begin=rng[0], root_end=rng[1],
+                      timeout_ms=um_timeout_ms if name == "um_only" else args.timeout_s * 1000)
+            if split is not None:
+                kw["cold_cache"] = 1
+            times, st = [], None
+            try:
+                for k in range(1 + args.steps):
+                    c, st = ctx.match(g, [p], **kw)
+                    if want is None:
+                        want = c[0]
+                    if c[0] != want:
+                        raise RuntimeError(f"{name}: count {c[0]} differs from {want}")
+                    if k >= 1:
+                        times.append(st["kernel_ms"])
+            except pm.PmError as e:
+                if e.status != pm.PM_ERR_TIMEOUT:
+                    raise
+                rows[name] = {"timed_out_ms": kw["timeout_ms"]}
+                continue
+            info = g.info()
+            row = {"kernel_ms": statistics.median(times)}
+            if split is not None:
+                row.update(frames=int(info["n_frames"]), static_frames=int(info["n_static_frames"]),
+                           pages=int(info["n_pages"]), page_hits=st["page_hits"], page_misses=st["page_misses"],
+                           pages_loaded=st["pages_loaded"] + st["device_page_loads"],
+                           zero_copy_bytes=st["zero_copy_bytes"], h2d_page_bytes=st["h2d_page_bytes"])
+            rows[name] = row
+        finally:
+            g.close()
+    ctx.close()
+    return {"workload": workload, "root_range": list(rng), "page_bytes": pb, "count": want, "counts_equal": True,
+            "arms": rows}
+
+
+def page_size_tuning(args, workload="rmat128k_batch20_lab32", root_share=8):
+    """The autotuner's page-size axis on the batched query, paged: the twenty
+    patterns in one launch through a frame pool of half the adjacency (all
+    evictable), every run cold, at pages of 16, 64 and 256 KB with the
+    default launch configuration, over the first 1/root_share of the
+    shortest root list.  The tuner refuses a page size that changes a count."""
+    import torch
+
+    from pumatch_b200 import autotune
+    torch.cuda.set_device(0)
+    ctx = pm.Context(0)
+    w, hg, texts = build_workload(workload)
+    labeled = w["labeled"]
+    plans = [pm.PatternPreprocessor(text=t, labeled=labeled) for _, t in texts]
+    g0 = pm.GraphPreprocessor.from_host(hg, labeled=labeled, device=0)
+    shortest = min(ctx.count_roots(g0, p) for p in plans)
+    g0.close()
+    rng = dict(root_begin=0, root_end=max(1, shortest // root_share))
+    pool = hg.colidx.nbytes // 2
+    out = autotune.autotune(ctx, hg, plans, labeled=labeled, paged=True, frame_pool_bytes=pool,
+                            page_kb=autotune.PAGE_KB, warps=(8,), chunks=(16,), splits=(64,), variants=(),
+                            reps=2, extra=rng, timeout_ms=args.timeout_s * 1000)
+    ctx.close()
+    return {"workload": workload, "patterns": len(plans), "root_range": [rng["root_begin"], rng["root_end"]],
+            "frame_pool_bytes": pool, "best_page_kb": out["best"]["page_kb"],
+            "kernel_ms_by_page_kb": {str(r["page_kb"]): r["kernel_ms"] for r in out["results"]},
+            "counts_equal": True}
+
+
 def comparisons(args):
     """The two comparisons the metric names, for the default line: the
     20-pattern batch in one launch vs one launch per pattern, and learned vs
@@ -827,6 +929,15 @@ def comparisons(args):
             "counts_equal": True, "plain": ln["plain"], "learned": ln["learned"]}
     except Exception as e:  # noqa: BLE001
         out["learned_vs_plain"] = {"error": f"{type(e).__name__}: {e}"[:300]}
+    try:
+        sub.steps = 2
+        out["paging_ablation"] = paging_ablation(sub)
+    except Exception as e:  # noqa: BLE001
+        out["paging_ablation"] = {"error": f"{type(e).__name__}: {e}"[:300]}
+    try:
+        out["page_size_tuning"] = page_size_tuning(sub)
+    except Exception as e:  # noqa: BLE001
+        out["page_size_tuning"] = {"error": f"{type(e).__name__}: {e}"[:300]}
     return out
 
 

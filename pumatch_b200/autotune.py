@@ -69,16 +69,20 @@ def sweep(ctx: Context, graph: GraphPreprocessor, plans: Sequence[PatternPreproc
 
 def autotune(ctx: Context, hg: HostGraph, plans: Sequence[PatternPreprocessor], *, labeled: bool,
              paged: bool = False, frame_pool_bytes: int = 4 << 30, page_kb: Iterable[int] = PAGE_KB,
-             out_json: Optional[str] = None, **kw) -> dict:
-    """Full sweep (page sizes too when paged); returns and optionally writes the best config."""
+             out_json: Optional[str] = None, extra: Optional[dict] = None, **kw) -> dict:
+    """Full sweep (page sizes too when paged); returns and optionally writes
+    the best config.  extra: run options every configuration shares (a root
+    range, say); paged sweeps start each run cold."""
     results = []
     for pk in (page_kb if paged else (None,)):
         g = GraphPreprocessor.from_host(hg, labeled=labeled, device=ctx.device, paged=paged,
                                         frame_pool_bytes=frame_pool_bytes,
                                         page_bytes=(pk << 10) if pk else 64 << 10)
         try:
-            extra = {"cold_cache": True} if paged else {}
-            for r in sweep(ctx, g, plans, extra=extra, **kw):
+            shared = dict(extra or {})
+            if paged:
+                shared["cold_cache"] = True
+            for r in sweep(ctx, g, plans, extra=shared, **kw):
                 r["page_kb"] = pk
                 results.append(r)
         finally:
