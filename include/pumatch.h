@@ -107,6 +107,59 @@ pm_status pm_graph_get_info(const pm_graph* g, pm_graph_info* info);
 pm_status pm_graph_set_resident_pages(pm_graph* g, const int64_t* pages, int64_t n);
 void pm_graph_close(pm_graph* g);
 
+/* Partitioned residency across the GPUs of one node.  Replaces the
+ * reference's placement of the edges beyond its device partition in host
+ * memory (test.cu:22-43, src/buffer.cu:986-1060) and its multi-node mode's
+ * full copy of the graph on every rank (test_mpi.cu:317-349): the adjacency
+ * array is cut into slices, each held once in the HBM of one GPU, and every
+ * GPU maps all slices into one device address range, which a paged graph
+ * takes its pages from (pm_graph_from_paged_source) instead of pinned host
+ * memory -- a miss is copied from the owner's HBM over NVLink.
+ *
+ * A pm_parts is such a range as one device sees it.  Slice p covers bytes
+ * [part_begin[p], part_begin[p+1]) (the last up to total_bytes); every
+ * boundary and total_bytes are multiples of pm_parts_granularity.  A slice is
+ * backed by new memory on a device of this process (pm_parts_alloc; it can be
+ * exported as a POSIX file descriptor for another process) or by memory
+ * another process exported (pm_parts_import).  pm_parts_map maps them all;
+ * pm_parts_ptr is then the range's device address (NULL before).  Slices
+ * allocated here are filled by the caller after mapping (pm_parts_write, or
+ * cudaMemcpy to pm_parts_ptr + part_begin[p]).  pm_parts_free unmaps and
+ * releases; memory exported to other processes lives until they release it
+ * too. */
+typedef struct pm_parts pm_parts;
+pm_status pm_parts_granularity(int device, uint64_t* bytes);
+pm_status pm_parts_create(int device, int n_parts, const uint64_t* part_begin, uint64_t total_bytes,
+                          pm_parts** out);
+pm_status pm_parts_alloc(pm_parts* r, int p, int owner_device);
+pm_status pm_parts_export(const pm_parts* r, int p, int* fd);
+pm_status pm_parts_import(pm_parts* r, int p, int fd);
+pm_status pm_parts_map(pm_parts* r);
+void* pm_parts_ptr(const pm_parts* r);
+/* Copies host bytes to [offset, offset + bytes) of a mapped range (a slice of
+ * this process, usually). */
+pm_status pm_parts_write(pm_parts* r, uint64_t offset, const void* host, uint64_t bytes);
+void pm_parts_free(pm_parts* r);
+
+/* A paged graph whose pages are cut from a device-visible array instead of
+ * pinned host memory (a pm_parts range; any device address this device can
+ * read).  src holds the paged layout: the adjacency array itself when
+ * unlabeled, its label-grouped copy when labeled (pm_label_group_host).
+ * sorted is the id-sorted array (labeled graphs read whole sorted lists from
+ * it in place; NULL for unlabeled graphs, where it is src).  Both must stay
+ * mapped until pm_graph_close; the graph does not own them.  opts as for
+ * pm_graph_from_host (residency is paged whatever opts says). */
+pm_status pm_graph_from_paged_source(int64_t n, int64_t n_adj, const uint64_t* rowptr,
+                                     const uint32_t* labels, const int32_t* src,
+                                     const int32_t* sorted, const pm_graph_opts* opts,
+                                     pm_graph** out);
+
+/* Host copy of the label-grouped layout a labeled paged graph caches: every
+ * list stably sorted by label (ids ascending within a label); out: n_adj
+ * int32.  labels are < 32. */
+pm_status pm_label_group_host(int64_t n, int64_t n_adj, const uint64_t* rowptr, const int32_t* colidx,
+                              const uint32_t* labels, int32_t* out);
+
 /* Reader/writer of the reference's on-disk layout (src/graph.h:228-254,
  * graph_converter/compactify.cpp:40-48, labelize.cpp:41-50) for host arrays.
  * pm_graph_read allocates *rowptr/*colidx/*labels with malloc; free with

@@ -142,6 +142,17 @@ SIGNATURES = {
     "pm_mlp_set_weights": (C.c_int, [_P, _P]),
     "pm_match_static": (C.c_int, [_P, _P, _P, C.c_int64, C.c_int64, C.c_int32, _P, C.POINTER(RunOpts), _P,
                                   C.POINTER(C.c_uint64), C.POINTER(Stats)]),
+    "pm_parts_granularity": (C.c_int, [C.c_int, C.POINTER(C.c_uint64)]),
+    "pm_parts_create": (C.c_int, [C.c_int, C.c_int, _P, C.c_uint64, _PP]),
+    "pm_parts_alloc": (C.c_int, [_P, C.c_int, C.c_int]),
+    "pm_parts_export": (C.c_int, [_P, C.c_int, C.POINTER(C.c_int)]),
+    "pm_parts_import": (C.c_int, [_P, C.c_int, C.c_int]),
+    "pm_parts_map": (C.c_int, [_P]),
+    "pm_parts_ptr": (C.c_void_p, [_P]),
+    "pm_parts_write": (C.c_int, [_P, C.c_uint64, _P, C.c_uint64]),
+    "pm_parts_free": (None, [_P]),
+    "pm_graph_from_paged_source": (C.c_int, [C.c_int64, C.c_int64, _P, _P, _P, _P, C.POINTER(GraphOpts), _PP]),
+    "pm_label_group_host": (C.c_int, [C.c_int64, C.c_int64, _P, _P, _P, _P]),
     "pm_strerror": (C.c_char_p, [C.c_int]),
     "pm_last_error": (C.c_char_p, []),
 }
@@ -386,6 +397,26 @@ class GraphPreprocessor:
                                           C.c_void_p(labels_ptr) if labels_ptr else None, device, C.byref(h)))
         return cls(_handle=h)
 
+    @classmethod
+    def from_paged_source(cls, hg: HostGraph, src_ptr: int, sorted_ptr: Optional[int] = None, *,
+                          labeled: bool = False, device: int = 0, frame_pool_bytes: int = 4 << 30,
+                          page_bytes: int = 64 << 10, static_pool_bytes: int = 0,
+                          keep_alive=None) -> "GraphPreprocessor":
+        """A paged graph whose pages come from a device-visible array (a
+        partitioned range, pumatch_b200.parts) instead of pinned host memory.
+        src_ptr: the paged layout (label-grouped when labeled); sorted_ptr:
+        the id-sorted array (labeled graphs).  keep_alive: objects that must
+        outlive the graph (the ranges the pointers come from)."""
+        o = cls._opts(labeled, device, True, frame_pool_bytes, page_bytes, static_pool_bytes)
+        h = C.c_void_p()
+        _check(lib().pm_graph_from_paged_source(hg.n, hg.n_adj, _ptr(hg.rowptr),
+                                                _ptr(hg.labels) if labeled else None, C.c_void_p(src_ptr),
+                                                C.c_void_p(sorted_ptr) if sorted_ptr else None, C.byref(o),
+                                                C.byref(h)))
+        g = cls(_handle=h)
+        g._keep = keep_alive
+        return g
+
     def info(self) -> dict:
         gi = GraphInfo()
         _check(lib().pm_graph_get_info(self._h, C.byref(gi)))
@@ -400,6 +431,7 @@ class GraphPreprocessor:
         if self._h:
             lib().pm_graph_close(self._h)
             self._h = None
+        self._keep = None
 
     def __del__(self):
         try:

@@ -25,7 +25,7 @@ NVCC = os.path.join(CUDA, "bin", "nvcc")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CU_SOURCES = ["pm_device.cu", "pm_paging.cu", "pm_learn.cu", "pm_gen.cu"]
-CPP_SOURCES = ["pm_host.cpp"]
+CPP_SOURCES = ["pm_host.cpp", "pm_parts.cpp"]
 HEADERS = ["pm_common.h", "pm_device.cuh"]
 
 

@@ -1956,13 +1956,17 @@ static pm_status graph_finish(pm_graph* g) {
 
 // Labeled paged graphs: the label-grouped copy of the adjacency array goes to
 // pinned host memory (it is what the frames cache), the group offsets to the
-// device.  Grouped on the device from the host array, a vertex range at a
-// time through a bounded device buffer.
-static pm_status paged_group_labels(pm_graph* g, const uint64_t* h_rowptr) {
+// device.  Grouped on the device from the id-sorted array (h_colidx_dev), a
+// vertex range at a time through a bounded device buffer.  With keep_copy
+// false only the offsets are kept: the caller's source holds the grouped
+// layout already (pm_graph_from_paged_source).
+static pm_status paged_group_labels(pm_graph* g, const uint64_t* h_rowptr, bool keep_copy = true) {
   g->nl1 = (g->nlabels > 0 ? g->nlabels : 32) + 1;
-  CK(cudaHostAlloc((void**)&g->h_colidx_lab, sizeof(int32_t) * std::max<int64_t>(g->nadj, 1),
-                   cudaHostAllocMapped | cudaHostAllocPortable));
-  CK(cudaHostGetDevicePointer((void**)&g->h_colidx_lab_dev, g->h_colidx_lab, 0));
+  if (keep_copy) {
+    CK(cudaHostAlloc((void**)&g->h_colidx_lab, sizeof(int32_t) * std::max<int64_t>(g->nadj, 1),
+                     cudaHostAllocMapped | cudaHostAllocPortable));
+    CK(cudaHostGetDevicePointer((void**)&g->h_colidx_lab_dev, g->h_colidx_lab, 0));
+  }
   CK(cudaMalloc(&g->d_lab_off, sizeof(int32_t) * (size_t)std::max<int64_t>(g->n, 1) * g->nl1));
   g->device_bytes += sizeof(int32_t) * (size_t)g->n * g->nl1;
   const int64_t chunk = std::max<int64_t>(g->maxdeg, std::min<int64_t>(std::max<int64_t>(g->nadj, 1), 64ll << 20));
@@ -1977,19 +1981,23 @@ static pm_status paged_group_labels(pm_graph* g, const uint64_t* h_rowptr) {
     label_group_kernel<<<2048, 256>>>(g->d_rowptr, g->h_colidx_dev, g->d_labels, v0, v1, g->nl1, tmp, b0,
                                       g->d_lab_off);
     cudaError_t e = cudaGetLastError();
-    if (e == cudaSuccess && len) e = cudaMemcpy(g->h_colidx_lab + b0, tmp, sizeof(int32_t) * len, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && len && keep_copy)
+      e = cudaMemcpy(g->h_colidx_lab + b0, tmp, sizeof(int32_t) * len, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && !keep_copy) e = cudaDeviceSynchronize();
     if (e != cudaSuccess) st = fail(PM_ERR_CUDA, "label grouping: %s", cudaGetErrorString(e));
     v0 = v1;
   }
   cudaFree(tmp);
   if (st != PM_OK) return st;
-  g->h_paged = g->h_colidx_lab;
-  g->h_paged_dev = g->h_colidx_lab_dev;
+  if (keep_copy) {
+    g->h_paged = g->h_colidx_lab;
+    g->h_paged_dev = g->h_colidx_lab_dev;
+  }
   return PM_OK;
 }
 
 namespace pm {
-pm_status paged_place(pm_graph* g, const int32_t* colidx, const pm_graph_opts* o);
+pm_status paged_place(pm_graph* g, const int32_t* colidx, const pm_graph_opts* o, const int32_t* src_dev);
 pm_status paged_maxnbrdeg(pm_graph* g);
 void paged_release(pm_graph* g);
 pm_status paged_prepare(pm_ctx* ctx, pm_graph* g, bool cold, DPaging* out);
@@ -2008,17 +2016,10 @@ extern "C" void pm_graph_opts_default(pm_graph_opts* o) {
   o->frame_pool_bytes = 4ull << 30;
 }
 
-extern "C" pm_status pm_graph_from_host(int64_t n, int64_t nadj, const uint64_t* rowptr, const int32_t* colidx,
-                                        const uint32_t* labels, const pm_graph_opts* opts, pm_graph** out) {
-  if (!rowptr || (nadj > 0 && !colidx) || !out || n < 0 || n > INT32_MAX - 1)
-    return fail(PM_ERR_INVALID, "pm_graph_from_host: bad arguments");
-  pm_graph_opts o;
-  pm_graph_opts_default(&o);
-  if (opts) o = *opts;
-  pm_status st = check_device(o.device);
-  if (st != PM_OK) return st;
-  if (o.labeled && !labels) return fail(PM_ERR_INVALID, "labeled graph without labels");
-  std::unique_ptr<pm_graph> g(new pm_graph);
+// The row offsets and labels of a graph placed from host arrays, on the
+// device (every residency).
+static pm_status place_rows(pm_graph* g, int64_t n, int64_t nadj, const uint64_t* rowptr, const uint32_t* labels,
+                            const pm_graph_opts& o) {
   g->device = o.device;
   g->n = n;
   g->nadj = nadj;
@@ -2043,8 +2044,24 @@ extern "C" pm_status pm_graph_from_host(int64_t n, int64_t nadj, const uint64_t*
     CK(cudaMemcpy(g->d_labels, lab.data(), n, cudaMemcpyHostToDevice));
     g->device_bytes += n;
   }
+  return PM_OK;
+}
+
+extern "C" pm_status pm_graph_from_host(int64_t n, int64_t nadj, const uint64_t* rowptr, const int32_t* colidx,
+                                        const uint32_t* labels, const pm_graph_opts* opts, pm_graph** out) {
+  if (!rowptr || (nadj > 0 && !colidx) || !out || n < 0 || n > INT32_MAX - 1)
+    return fail(PM_ERR_INVALID, "pm_graph_from_host: bad arguments");
+  pm_graph_opts o;
+  pm_graph_opts_default(&o);
+  if (opts) o = *opts;
+  pm_status st = check_device(o.device);
+  if (st != PM_OK) return st;
+  if (o.labeled && !labels) return fail(PM_ERR_INVALID, "labeled graph without labels");
+  std::unique_ptr<pm_graph> g(new pm_graph);
+  st = place_rows(g.get(), n, nadj, rowptr, labels, o);
+  if (st != PM_OK) return st;
   if (o.residency == PM_RESIDENT_PAGED) {
-    st = paged_place(g.get(), colidx, &o);
+    st = paged_place(g.get(), colidx, &o, nullptr);
     if (st != PM_OK) return st;
     CK(cudaMalloc(&g->d_maxnbrdeg, sizeof(int32_t) * std::max<int64_t>(g->n, 1)));
     g->device_bytes += sizeof(int32_t) * g->n;
@@ -2059,6 +2076,44 @@ extern "C" pm_status pm_graph_from_host(int64_t n, int64_t nadj, const uint64_t*
     if (nadj) CK(cudaMemcpy(g->d_colidx, colidx, sizeof(int32_t) * nadj, cudaMemcpyHostToDevice));
     g->device_bytes += sizeof(int32_t) * nadj;
     st = graph_finish(g.get());
+    if (st != PM_OK) return st;
+  }
+  *out = g.release();
+  return PM_OK;
+}
+
+extern "C" pm_status pm_graph_from_paged_source(int64_t n, int64_t nadj, const uint64_t* rowptr,
+                                                const uint32_t* labels, const int32_t* src, const int32_t* sorted,
+                                                const pm_graph_opts* opts, pm_graph** out) {
+  if (!rowptr || !out || n < 0 || n > INT32_MAX - 1 || nadj < 0 || (nadj > 0 && !src))
+    return fail(PM_ERR_INVALID, "pm_graph_from_paged_source: bad arguments");
+  pm_graph_opts o;
+  pm_graph_opts_default(&o);
+  if (opts) o = *opts;
+  o.residency = PM_RESIDENT_PAGED;
+  if (o.labeled && (!labels || (nadj > 0 && !sorted)))
+    return fail(PM_ERR_INVALID, "a labeled graph needs labels and the id-sorted array");
+  if (!o.labeled) sorted = src;
+  if (rowptr[n] != (uint64_t)nadj)
+    return fail(PM_ERR_INVALID, "rowptr[n] = %llu but n_adj = %lld", (unsigned long long)rowptr[n], (long long)nadj);
+  if (((uintptr_t)src & 15) || ((uintptr_t)sorted & 15))
+    return fail(PM_ERR_INVALID, "the source arrays must be 16-byte aligned");
+  pm_status st = check_device(o.device);
+  if (st != PM_OK) return st;
+  std::unique_ptr<pm_graph> g(new pm_graph);
+  st = place_rows(g.get(), n, nadj, rowptr, labels, o);
+  if (st != PM_OK) return st;
+  st = paged_place(g.get(), nullptr, &o, src);
+  if (st != PM_OK) return st;
+  // the id-sorted lists: root filter, features, and a labeled graph's whole
+  // lists (read in place)
+  g->h_colidx_dev = const_cast<int32_t*>(sorted);
+  CK(cudaMalloc(&g->d_maxnbrdeg, sizeof(int32_t) * std::max<int64_t>(g->n, 1)));
+  g->device_bytes += sizeof(int32_t) * g->n;
+  st = paged_maxnbrdeg(g.get());
+  if (st != PM_OK) return st;
+  if (g->labeled && n > 0) {
+    st = paged_group_labels(g.get(), rowptr, false);
     if (st != PM_OK) return st;
   }
   *out = g.release();

@@ -89,6 +89,12 @@ static void release_state(PagedState* s) {
   delete s;
 }
 
+// Copies out of the page source: pinned host memory, or (a graph placed on
+// an external source) device memory of this or another GPU.
+static cudaMemcpyKind source_kind(const pm_graph* g) {
+  return g->h_colidx ? cudaMemcpyHostToDevice : cudaMemcpyDefault;
+}
+
 // Resets the table to the initial residency (frames 0..prefilled-1 hold the
 // pages init_fp names), or, when cold, to the static frames alone.  Evictable
 // initial pages are recopied into their frames every time, since the last run
@@ -104,6 +110,7 @@ static pm_status reset_table(pm_graph* g, cudaStream_t st, bool cold) {
   CKP(cudaMemcpyAsync(s->frame_state, s->fs_host, sizeof(unsigned long long) * g->n_frames,
                       cudaMemcpyHostToDevice, st));
   const size_t pb = (size_t)g->page_ints * 4;
+  const cudaMemcpyKind kind = source_kind(g);
   for (int64_t f = s->static_loaded ? s->n_static : 0; f < pre;) {
     // coalesce runs of consecutive pages in consecutive frames into one copy
     // (a run never crosses the static boundary)
@@ -111,7 +118,7 @@ static pm_status reset_table(pm_graph* g, cudaStream_t st, bool cold) {
     while (e < pre && e != s->n_static && fp[e] == fp[e - 1] + 1) e++;
     const int64_t first = (int64_t)fp[f] * g->page_ints;
     const size_t bytes = std::min<size_t>((size_t)(e - f) * pb, sizeof(int32_t) * (size_t)(g->nadj - first));
-    CKP(cudaMemcpyAsync((char*)s->frames + (size_t)f * pb, g->h_paged + first, bytes, cudaMemcpyHostToDevice, st));
+    CKP(cudaMemcpyAsync((char*)s->frames + (size_t)f * pb, g->h_paged + first, bytes, kind, st));
     f = e;
   }
   CKP(cudaMemsetAsync(s->frame_ref, 0, g->n_frames, st));
@@ -152,7 +159,10 @@ static pm_status set_initial(pm_graph* g, std::vector<int64_t> pages) {
   return PM_OK;
 }
 
-pm_status paged_place(pm_graph* g, const int32_t* colidx, const pm_graph_opts* o) {
+// Places a paged graph.  The pages are cut from src_dev when it is given (a
+// device-visible array: another GPU's HBM through a pm_parts range, say),
+// else from a pinned, mapped host copy of colidx.
+pm_status paged_place(pm_graph* g, const int32_t* colidx, const pm_graph_opts* o, const int32_t* src_dev) {
   uint32_t pb = o->page_bytes ? o->page_bytes : (64u << 10);
   if (pb < 4096 || (pb & (pb - 1))) return fail(PM_ERR_INVALID, "page_bytes must be a power of two >= 4096");
   std::unique_ptr<PagedState> s(new PagedState);
@@ -164,20 +174,25 @@ pm_status paged_place(pm_graph* g, const int32_t* colidx, const pm_graph_opts* o
   g->n_pages = (nadj + g->page_ints - 1) / g->page_ints;
   g->n_frames = std::min<int64_t>((int64_t)(o->frame_pool_bytes / pb), g->n_pages);
   if (g->n_frames < 1 && g->n_pages > 0) g->n_frames = 1;
-  // adjacency in pinned, mapped host memory
-  CKP(cudaHostAlloc((void**)&g->h_colidx, sizeof(int32_t) * std::max<int64_t>(nadj, 1),
-                    cudaHostAllocMapped | cudaHostAllocPortable));
-  if (nadj) {
-    const int64_t kBlock = 1 << 24;
+  if (src_dev) {
+    // an external source: nothing to copy; the caller keeps it mapped
+    g->h_paged = g->h_paged_dev = src_dev;
+  } else {
+    // adjacency in pinned, mapped host memory
+    CKP(cudaHostAlloc((void**)&g->h_colidx, sizeof(int32_t) * std::max<int64_t>(nadj, 1),
+                      cudaHostAllocMapped | cudaHostAllocPortable));
+    if (nadj) {
+      const int64_t kBlock = 1 << 24;
 #pragma omp parallel for schedule(static)
-    for (int64_t b = 0; b < (nadj + kBlock - 1) / kBlock; b++) {
-      const int64_t e = std::min(nadj, (b + 1) * kBlock);
-      memcpy(g->h_colidx + b * kBlock, colidx + b * kBlock, sizeof(int32_t) * (e - b * kBlock));
+      for (int64_t b = 0; b < (nadj + kBlock - 1) / kBlock; b++) {
+        const int64_t e = std::min(nadj, (b + 1) * kBlock);
+        memcpy(g->h_colidx + b * kBlock, colidx + b * kBlock, sizeof(int32_t) * (e - b * kBlock));
+      }
     }
+    CKP(cudaHostGetDevicePointer((void**)&g->h_colidx_dev, g->h_colidx, 0));
+    g->h_paged = g->h_colidx;  // a labeled graph switches to its label-grouped copy after placement
+    g->h_paged_dev = g->h_colidx_dev;
   }
-  CKP(cudaHostGetDevicePointer((void**)&g->h_colidx_dev, g->h_colidx, 0));
-  g->h_paged = g->h_colidx;  // a labeled graph switches to its label-grouped copy after placement
-  g->h_paged_dev = g->h_colidx_dev;
   // device page table and frame pool
   const size_t fbytes = (size_t)g->n_frames * pb;
   CKP(cudaMalloc(&s->frames, std::max<size_t>(fbytes, 4)));
@@ -283,7 +298,7 @@ static void service_loop(pm_graph* g) {
       const int64_t first = (int64_t)req.x * g->page_ints;
       const size_t bytes = std::min<size_t>(pb, sizeof(int32_t) * (size_t)(nadj - first));
       cudaError_t e = cudaMemcpyAsync((char*)s->frames + (size_t)req.y * pb, g->h_paged + first, bytes,
-                                      cudaMemcpyHostToDevice, s->copy_stream);
+                                      source_kind(g), s->copy_stream);
       if (e == cudaSuccess)
         e = cudaMemcpyAsync(s->page_frame + req.x, s->stage + req.y, sizeof(int32_t), cudaMemcpyHostToDevice,
                             s->copy_stream);
