@@ -443,6 +443,10 @@ def run_ours(args, workload):
         order_h = torch.tensor(ids, dtype=torch.int32).pin_memory()
         order = order_h.to("cuda")
         run_kw.update(root_order_ptr=order.data_ptr(), root_begin=0, root_end=len(order_h))
+        if world > 1:
+            # a sample of a few roots: one root per chunk, so that the
+            # chunk-cyclic shards spread them over the ranks
+            run_kw["chunk"] = 1
 
     def one_step():
         with torch.cuda.stream(stream):
