@@ -156,7 +156,9 @@ pm_status pm_graph_from_paged_source(int64_t n, int64_t n_adj, const uint64_t* r
 
 /* Host copy of the label-grouped layout a labeled paged graph caches: every
  * list stably sorted by label (ids ascending within a label); out: n_adj
- * int32.  labels are < 32. */
+ * int32.  labels are < 32.  No counterpart in the reference, which tests
+ * each element's label inside its set operation (src/gpu_match.cu:238-319);
+ * the grouping changes which elements are read, not the counts. */
 pm_status pm_label_group_host(int64_t n, int64_t n_adj, const uint64_t* rowptr, const int32_t* colidx,
                               const uint32_t* labels, int32_t* out);
 
