@@ -213,6 +213,15 @@ def place_graph(w, hg, device):
     else:  # a share of the adjacency array
         pool = max(pb, int(hg.colidx.nbytes * pg["frame_fraction"]) // pb * pb)
         static = int(hg.colidx.nbytes * pg.get("static_fraction", 0.0)) // pb * pb
+    if pg.get("partitioned"):
+        # the array cut into slices held in the HBM of this node's GPUs (all
+        # on `device` when it is the only one), mapped into one device range
+        import torch
+
+        from pumatch_b200 import parts
+        k, ndev = pg["partitioned"], max(1, torch.cuda.device_count())
+        return parts.place_local(hg, k, device=device, owners=[(device + i) % ndev for i in range(k)],
+                                 labeled=w["labeled"], frame_pool_bytes=pool, page_bytes=pb, static_pool_bytes=static)
     return pm.GraphPreprocessor.from_host(hg, labeled=w["labeled"], device=device, paged=True,
                                           page_bytes=pb, frame_pool_bytes=pool, static_pool_bytes=static)
 
@@ -399,6 +408,8 @@ def run_ours(args, workload):
     if args.static_frac is not None and w.get("paged") and "frame_bytes" in w["paged"]:
         # part of the absolute pool placed once and never evicted (the array's first pages)
         w = dict(w, paged=dict(w["paged"], static_bytes=int(args.static_frac * w["paged"]["frame_bytes"])))
+    if args.partitioned and w.get("paged"):
+        w = dict(w, paged=dict(w["paged"], partitioned=args.partitioned))
     sample = load_sample(w, hg, args.samples)
     subset = bool(sample and sample.get("extra_roots"))
     if sample is not None and args.sample_roots:
@@ -606,6 +617,10 @@ def run_ours(args, workload):
                 "zero_copy_bytes_last_step": int(st["zero_copy_bytes"]),
                 "achieved_gbs": link / (st["kernel_ms"] / 1000.0) / 1e9 if st["kernel_ms"] > 0 else 0.0,
                 "nominal_gbs": 64.0, "nominal": "PCIe Gen5 x16, one direction"}
+            if w["paged"].get("partitioned"):
+                line["host_link"].update(
+                    source=f"array partitioned into {w['paged']['partitioned']} slices of device memory",
+                    nominal_gbs=900.0, nominal="NVLink 5, one direction (peer slices; local slices read from HBM)")
         if world == 1 and not args.no_cpu_baseline:
             threads = os.cpu_count() or 1
             cm = cpu_measure(hg, texts, labeled, threads, sample, time_limit_s=15.0, per_root=sample is None)
@@ -994,6 +1009,9 @@ def main():
                     help="kernel variant: 0 default, 1 capped at 64 registers, 2 capped at 85, 3 uncapped")
     ap.add_argument("--static-frac", type=float, default=None,
                     help="paged workloads with an absolute pool: this share of it static (never evicted)")
+    ap.add_argument("--partitioned", type=int, default=0,
+                    help="paged workloads: take pages from the array cut into this many slices of device memory "
+                         "(one per GPU of the node, round robin) instead of pinned host memory")
     ap.add_argument("--host-page-copy", action="store_true",
                     help="paged: every page load through the host service thread (no warp-side copies)")
     ap.add_argument("--leaf-per-lane", type=int, default=0,
