@@ -255,7 +255,10 @@ def exchange_fds(job: str, rank: int, world: int, mine: Dict[int, int], timeout_
                     time.sleep(0.01)
             with s:
                 # header and keys in one message, with every descriptor attached
-                socket.send_fds(s, [payload], [mine[k] for k in keys])
+                if keys:
+                    socket.send_fds(s, [payload], [mine[k] for k in keys])
+                else:
+                    s.sendall(payload)
         th.join(max(0.0, deadline - time.monotonic()) + 1.0)
         if th.is_alive():
             raise TimeoutError("peers did not send their descriptors in time")
