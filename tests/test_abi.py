@@ -77,6 +77,14 @@ def test_no_cpu_fallback():
     with pytest.raises(pm.PmError) as e:
         pm.GraphPreprocessor.from_host(hg)
     assert e.value.status == pm.PM_ERR_NO_DEVICE
+    # partitioned residency: no device range without a device
+    from pumatch_b200 import parts
+    with pytest.raises(pm.PmError) as e:
+        parts.granularity(0)
+    assert e.value.status == pm.PM_ERR_NO_DEVICE
+    with pytest.raises(pm.PmError) as e:
+        pm.GraphPreprocessor.from_paged_source(hg, 1 << 20)  # refused before the pointer is used
+    assert e.value.status == pm.PM_ERR_NO_DEVICE
     # the drop-in CLI fails loudly too
     gold = os.path.join(ROOT, "tests", "golden", "graphs", "cl400")
     pat = os.path.join(ROOT, "tests", "golden", "_c4.g")
