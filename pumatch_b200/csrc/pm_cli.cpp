@@ -3,7 +3,7 @@
 //   test <graph-prefix> <pattern.g> [--labeled=0|1] [--truncate=N] [--device=D]
 //        [--paged] [--frame-mb=M] [--static-mb=S] [--page-kb=K] [--batch=<list file>]
 //        [--warps=W] [--chunk=C] [--split=S] [--variant=V] [--tuned=<autotuner json>]
-//        [--json=<path>]
+//        [--json=<path>] [--parts=K] [--parts-device=D]
 //
 // Same positional arguments and output as the reference's driver
 // (test.cu:15-21, 200-209): the last stdout line is "<kernel ms> <count>" and
@@ -19,6 +19,10 @@
 // chunk, split_level1, high_occupancy, page_kb); explicit flags after it
 // override it.  --variant picks the kernel's register cap (pm_run_opts
 // high_occupancy: 1 = 64, 2 = 85, 3 = uncapped; 0 = the default).
+// --parts=K pages the graph (as --paged, with its pool options) from the
+// adjacency array cut into K slices of device memory, slice p in the HBM of
+// GPU device+p (all on GPU D with --parts-device=D), mapped into one range:
+// partitioned residency, misses copied from the owner's HBM over NVLink.
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -53,11 +57,73 @@ static int die(const char* what, pm_status s) {
   return 1;
 }
 
+// Places the graph at `prefix` paged from k slices of device memory (see
+// --parts above); the ranges stay mapped until the caller frees them, after
+// the graph.  Slice bounds: multiples of the allocation granularity and of the
+// page size, equal slices but for the last (pumatch_b200/parts.py does the
+// same).
+static pm_status place_parts(const char* prefix, const pm_graph_opts& go, int k, int one_device,
+                             std::vector<pm_parts*>& ranges, pm_graph** out) {
+  int64_t n = 0, nadj = 0;
+  int32_t maxd = 0;
+  uint64_t* rowptr = nullptr;
+  int32_t* colidx = nullptr;
+  uint32_t* labels = nullptr;
+  pm_status s = pm_graph_read(prefix, go.labeled, &n, &nadj, &maxd, &rowptr, &colidx, &labels);
+  if (s != PM_OK) return s;
+  std::vector<int32_t> grouped;
+  std::vector<const int32_t*> arrays;
+  if (go.labeled) {
+    grouped.resize((size_t)nadj);
+    s = pm_label_group_host(n, nadj, rowptr, colidx, labels, grouped.data());
+    arrays = {grouped.data(), colidx};
+  } else {
+    arrays = {colidx};
+  }
+  uint64_t gran = 0;
+  if (s == PM_OK) s = pm_parts_granularity(go.device, &gran);
+  std::vector<uint64_t> begins;
+  uint64_t total = 0;
+  if (s == PM_OK) {
+    const uint64_t align = gran > go.page_bytes ? gran : go.page_bytes;
+    const uint64_t bytes = 4ull * (uint64_t)nadj;
+    uint64_t units = (bytes + align - 1) / align;
+    if (units == 0) units = 1;
+    const uint64_t per = (units + (uint64_t)k - 1) / (uint64_t)k;
+    for (uint64_t p = 0; p < (uint64_t)k && p * per < units; p++) begins.push_back(p * per * align);
+    total = units * align;
+  }
+  for (size_t a = 0; a < arrays.size() && s == PM_OK; a++) {
+    pm_parts* r = nullptr;
+    s = pm_parts_create(go.device, (int)begins.size(), begins.data(), total, &r);
+    if (s != PM_OK) break;
+    ranges.push_back(r);
+    for (size_t p = 0; p < begins.size() && s == PM_OK; p++)
+      s = pm_parts_alloc(r, (int)p, one_device >= 0 ? one_device : go.device + (int)p);
+    if (s == PM_OK) s = pm_parts_map(r);
+    for (size_t p = 0; p < begins.size() && s == PM_OK; p++) {
+      const uint64_t b = begins[p], e = p + 1 < begins.size() ? begins[p + 1] : total;
+      const uint64_t have = 4ull * (uint64_t)nadj;
+      if (b < have)
+        s = pm_parts_write(r, b, (const char*)arrays[a] + b, (e < have ? e : have) - b);
+    }
+  }
+  if (s == PM_OK)
+    s = pm_graph_from_paged_source(n, nadj, rowptr, go.labeled ? labels : nullptr,
+                                   (const int32_t*)pm_parts_ptr(ranges[0]),
+                                   go.labeled ? (const int32_t*)pm_parts_ptr(ranges[1]) : nullptr, &go, out);
+  pm_host_free(rowptr);
+  pm_host_free(colidx);
+  pm_host_free(labels);
+  return s;
+}
+
 int main(int argc, char** argv) {
   if (argc < 3) {
     fprintf(stderr, "usage: test <graph-prefix> <pattern.g> [--labeled=0|1] [--truncate=N] [--device=D]\n"
                     "            [--paged] [--frame-mb=M] [--static-mb=S] [--page-kb=K] [--batch=<list>]\n"
-                    "            [--warps=W] [--chunk=C] [--split=S] [--variant=V] [--tuned=<json>] [--json=<path>]\n");
+                    "            [--warps=W] [--chunk=C] [--split=S] [--variant=V] [--tuned=<json>] [--json=<path>]\n"
+                    "            [--parts=K] [--parts-device=D]\n");
     return 2;
   }
   const char* prefix = argv[1];
@@ -65,6 +131,7 @@ int main(int argc, char** argv) {
   int labeled = 1, truncate = 0, device = 0, paged = 0;
   long long frame_mb = 4096, static_mb = 0, page_kb = 64;
   long long warps = 0, chunk = 0, split = 0, variant = 0;
+  int n_parts = 0, parts_device = -1;
   std::string batch, json_path;
   for (int i = 3; i < argc; i++) {
     const char* a = argv[i];
@@ -93,6 +160,8 @@ int main(int argc, char** argv) {
     else if (!strncmp(a, "--static-mb=", 12)) static_mb = atoll(a + 12);
     else if (!strncmp(a, "--page-kb=", 10)) page_kb = atoll(a + 10);
     else if (!strncmp(a, "--batch=", 8)) batch = a + 8;
+    else if (!strncmp(a, "--parts=", 8)) n_parts = atoi(a + 8);
+    else if (!strncmp(a, "--parts-device=", 15)) parts_device = atoi(a + 15);
     else { fprintf(stderr, "test: unknown option %s\n", a); return 2; }
   }
   std::vector<std::string> files;
@@ -106,18 +175,23 @@ int main(int argc, char** argv) {
       if (!line.empty() && line[0] != '#') files.push_back(line);
   }
 
+  if (n_parts < 0 || n_parts > 1024 || (parts_device >= 0 && n_parts == 0)) {
+    fprintf(stderr, "test: --parts takes 1..1024 slices (and --parts-device needs it)\n");
+    return 2;
+  }
   pm_graph_opts go;
   pm_graph_opts_default(&go);
   go.labeled = labeled;
   go.device = device;
-  if (paged) {
+  if (paged || n_parts) {
     go.residency = PM_RESIDENT_PAGED;
     go.frame_pool_bytes = (uint64_t)frame_mb << 20;
     go.page_bytes = (uint32_t)(page_kb << 10);
     go.static_pool_bytes = (uint64_t)static_mb << 20;
   }
   pm_graph* g = nullptr;
-  pm_status s = pm_graph_open(prefix, &go, &g);
+  std::vector<pm_parts*> ranges;
+  pm_status s = n_parts ? place_parts(prefix, go, n_parts, parts_device, ranges, &g) : pm_graph_open(prefix, &go, &g);
   if (s != PM_OK) return die("graph", s);
   pm_graph_info gi;
   pm_graph_get_info(g, &gi);
@@ -175,5 +249,6 @@ int main(int argc, char** argv) {
   for (auto* p : plans) pm_plan_free(p);
   pm_ctx_destroy(ctx);
   pm_graph_close(g);
+  for (auto* r : ranges) pm_parts_free(r);
   return 0;
 }

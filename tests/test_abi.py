@@ -131,6 +131,27 @@ def test_cli_tuned_file_errors(tmp_path):
     assert r.returncode == 2
 
 
+def test_cli_parts_options():
+    """--parts (partitioned residency) is validated before anything runs, and
+    without a GPU the CLI fails loudly: no slice is ever placed in host
+    memory instead."""
+    gold = os.path.join(ROOT, "tests", "golden", "graphs", "cl400")
+    r = subprocess.run([pm.CLI_PATH], capture_output=True, text=True)
+    assert "--parts=K" in r.stderr
+    for bad in (["--parts-device=0"], ["--parts=-1"], ["--parts=5000"]):
+        r = subprocess.run([pm.CLI_PATH, gold, "x.g", *bad], capture_output=True, text=True)
+        assert r.returncode == 2 and "--parts" in r.stderr, bad
+    if not torch.cuda.is_available():
+        from pumatch_b200 import patterns as P
+        pat = os.path.join(ROOT, "tests", "golden", "_c4_parts.g")
+        open(pat, "w").write(P.to_g(*P.cycle(4)))
+        try:
+            r = subprocess.run([pm.CLI_PATH, gold, pat, "--parts=2"], capture_output=True, text=True)
+            assert r.returncode == 1 and "no CUDA device" in r.stderr
+        finally:
+            os.remove(pat)
+
+
 def test_run_option_keywords():
     """Every run option the bench, the tests and the learned/autotune helpers
     pass maps onto a pm_run_opts field; a misspelt one is an error, not a
