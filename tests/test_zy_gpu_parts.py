@@ -125,6 +125,22 @@ def test_three_slices_count_like_the_oracle(ctx, labeled, mode):
         g.close()
 
 
+def test_cli_parts_count_equals_hbm(tmp_path):
+    """The drop-in CLI with --parts prints the count the HBM placement
+    prints (the last stdout line, "<ms> <count>")."""
+    import subprocess
+    gold = os.path.join(GOLD, "graphs", "cl3000")
+    pat = tmp_path / "c5.g"
+    pat.write_text(P.to_g(*P.cycle(5), [0, 0, 1, 1, 0]))
+    counts = []
+    for extra in ([], ["--parts=2", "--parts-device=0", "--page-kb=4", "--frame-mb=1"]):
+        r = subprocess.run([pm.CLI_PATH, gold, str(pat), *extra], capture_output=True, text=True, cwd=tmp_path,
+                           timeout=300)
+        assert r.returncode == 0, r.stderr
+        counts.append(int(r.stdout.strip().splitlines()[-1].split()[1]))
+    assert counts[0] == counts[1] > 0
+
+
 def test_source_arguments_are_checked():
     hg = workload()
     with pytest.raises(pm.PmError):  # labeled without the id-sorted array
