@@ -141,3 +141,111 @@ def test_gloo_ranks_exchange_slice_descriptors(world):
 
 def test_single_rank_exchange_is_empty():
     assert parts.exchange_fds("solo", 0, 1, {0: 5}) == {}
+
+
+class _FakeRange:
+    """Stands in for a device range on CPU: a slice allocated here is a memfd,
+    exported as a duplicate descriptor; an imported slice keeps the peer's
+    descriptor.  Reading a slice reads what its owner wrote."""
+    log = None
+
+    def __init__(self, device, begins, total):
+        self.begins, self.total = list(begins), total
+        self.fds = {}
+        self.mapped = False
+
+    def bounds(self, p):
+        return self.begins[p], self.begins[p + 1] if p + 1 < len(self.begins) else self.total
+
+    def alloc(self, p, owner_device):
+        b, e = self.bounds(p)
+        fd = os.memfd_create(f"slice{p}")
+        os.ftruncate(fd, e - b)
+        self.fds[p] = fd
+
+    def export(self, p):
+        return os.dup(self.fds[p])
+
+    def import_(self, p, fd):
+        self.fds[p] = os.dup(fd)
+
+    def map(self):
+        assert sorted(self.fds) == list(range(len(self.begins))), "a slice has no memory"
+        self.mapped = True
+
+    @property
+    def ptr(self):
+        return id(self)
+
+    def fill_slice(self, p, array):
+        assert self.mapped
+        b, e = self.bounds(p)
+        raw = array.view(np.uint8)
+        os.pwrite(self.fds[p], raw[b:min(e, raw.nbytes)].tobytes(), 0)
+
+    def read_all(self, nbytes):
+        out = bytearray()
+        for p in range(len(self.begins)):
+            b, e = self.bounds(p)
+            out += os.pread(self.fds[p], e - b, 0)
+        return bytes(out[:nbytes])
+
+    def close(self):
+        for fd in self.fds.values():
+            os.close(fd)
+        self.fds = {}
+
+
+def _place_worker(rank, world, port, job, labeled, q):
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    sys.path.insert(0, root)
+    sys.path.insert(0, os.path.join(root, "tests"))
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    import torch.distributed as dist
+
+    import pumatch_b200 as pmm
+    from pumatch_b200 import parts as pp
+    import test_parts as t
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        hg = pmm.HostGraph.read(os.path.join(root, "tests", "golden", "graphs", "cl3000"), labeled=True)
+        seen = {}
+
+        def fake_place(hg_, src, srt, **kw):
+            ranges = kw["keep_alive"]
+            seen["views"] = [r.read_all(4 * hg_.n_adj) for r in ranges]
+            seen["ptrs"] = (src == ranges[0].ptr, srt == (ranges[1].ptr if kw["labeled"] else None))
+            return "graph"
+
+        pp.Range = t._FakeRange
+        pp.granularity = lambda device=0: 4096
+        pmm.GraphPreprocessor.from_paged_source = staticmethod(fake_place)
+        g = pp.place_distributed(hg, rank, world, job=job, device=0, barrier=dist.barrier, labeled=labeled,
+                                 page_bytes=4096)
+        want = [pp.label_grouped(hg).tobytes(), hg.colidx.tobytes()] if labeled else [hg.colidx.tobytes()]
+        q.put((rank, g == "graph" and seen["views"] == want and all(seen["ptrs"])))
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("labeled", [True, False], ids=["labeled", "unlabeled"])
+def test_gloo_distributed_placement_sees_every_slice_filled(labeled):
+    """place_distributed's order on three gloo ranks, with a memfd standing in
+    for each rank's slice: every rank allocates its own slice, imports the
+    others', and builds the graph only after every slice was written, seeing
+    each array whole."""
+    world = 3
+    ctx = mp.get_context("spawn")
+    q = ctx.SimpleQueue()
+    port = _free_port()
+    job = uuid.uuid4().hex[:12]
+    procs = [ctx.Process(target=_place_worker, args=(r, world, port, job, labeled, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(120)
+        assert p.exitcode == 0
+    got = dict(q.get() for _ in range(world))
+    assert all(got[r] for r in range(world)), got
